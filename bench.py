@@ -1,0 +1,325 @@
+#!/usr/bin/env python
+"""Benchmark of the batched k-clique engine on B200.
+
+Workload (the batched configuration): 10,000 independent seeded graphs,
+n log-uniform in [50, 5000], families ER (p ~ U[0.005, 0.05]), 4-block SBM
+(p_in 0.1, p_out 0.005) and ER + one planted clique of size 20-40, k uniform
+in [4, 12]; degree orientation; mode / unit / partition / encoding picked per
+graph by the engine's autotuner. One step = counting every graph of the
+batch exactly (CSR build, orientation and the captured counting launch).
+
+  value   graphs/s with the edge lists already in HBM (device-input API);
+  e2e     the same through the host API with page-locked host inputs,
+          host->device copies and the read-back of the counts inside the step;
+  plain   graphs/s of the one-graph-per-launch path on a sample of the batch;
+  cpu_baseline  the CPU oracle (OpenMP, all host threads) on a bounded sample.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+Under torchrun each rank counts its own batch (seed shifted by rank): weak
+scaling, no collective on the data path; the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "graphs/s, batched exact k-clique counts (10,000 mixed small graphs, k 4-12)"
+UNIT = "graphs/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--graphs", type=int, default=10000)
+    ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--plain-sample", type=int, default=400)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi during a region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg, device):
+    if pg is not None:
+        import torch
+
+        pg.barrier(device_ids=[device])
+        torch.cuda.synchronize()
+
+
+def max_over_ranks(pg, x: float, device) -> float:
+    if pg is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def make_batch(kc, n_graphs: int, seed: int):
+    el = kc.gen_batch(n_graphs, seed, pinned=True)
+    s, d, _ = el.arrays(copy=False)  # views of the page-locked arrays
+    off, nn, kk, fam = el.batch_meta()
+    return el, s, d, off, nn, kk, fam
+
+
+def cpu_oracle_sample(s, d, off, nn, kk, modes, budget_s: float):
+    """The CPU oracle on graphs 0, 1, ... until budget_s elapses; returns
+    (graphs done, seconds, counts)."""
+    from oracle.oracle import OracleGraph
+
+    counts = []
+    t0 = time.perf_counter()
+    g = 0
+    while g < len(nn) and time.perf_counter() - t0 < budget_s:
+        a, b = int(off[g]), int(off[g + 1])
+        og = OracleGraph(s[a:b], d[a:b], int(nn[g]))
+        og.orient("degree")
+        counts.append(og.count(int(kk[g]), mode="pivot" if modes[g] == 1 else "orient"))
+        g += 1
+    return g, time.perf_counter() - t0, counts
+
+
+def run_reference(args, world, rank, local, pg):
+    """The reference arm: KCGPU has no CPU counting path, so its CPU arm is the
+    oracle port (OpenMP, every host thread) on a bounded sample per step."""
+    if rank != 0:
+        return
+    import kcgpu_b200 as kc
+
+    from oracle.oracle import max_threads
+
+    el, s, d, off, nn, kk, fam = make_batch(kc, args.graphs, args.seed)
+    modes = [1 if (k >= 9 or f == 2) else 0 for k, f in zip(kk, fam)]
+    # size one step to ~12 s of CPU work on this host
+    probe, t_probe, _ = cpu_oracle_sample(s, d, off, nn, kk, modes, 3.0)
+    per_graph = t_probe / max(1, probe)
+    sample = int(max(1, min(args.graphs, 12.0 / max(per_graph, 1e-6))))
+    times = []
+    total = args.warmup + args.steps
+    for i in range(total):
+        done, dt, _ = cpu_oracle_sample(s, d, off[: sample + 1], nn[:sample], kk[:sample], modes, 1e9)
+        if i >= args.warmup:
+            times.append(dt)
+    mean = sum(times) / len(times)
+    val = sample / mean
+    line = {"metric": METRIC, "value": val, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64/u128 integer", "data": "synthetic (seeded)",
+            "config": {"workload": "batched: first %d of %d mixed graphs (ER / 4-block SBM / ER+planted clique), "
+                                   "n 50-5000, k 4-12, degree orientation" % (sample, args.graphs)},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": max_threads(), "kind": "port",
+                             "sample": f"first {sample} graphs of the batch per step"},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local, pg = dist_setup(args.gpus)
+    if args.impl == "reference":
+        run_reference(args, world, rank, local, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    import torch
+
+    torch.cuda.set_device(local)
+    import kcgpu_b200 as kc
+
+    ctx = kc.Context(local)
+    L = kc.lib()
+    el, s, d, off, nn, kk, fam = make_batch(kc, args.graphs, args.seed + rank * args.graphs)
+    G = len(nn)
+    E = int(off[-1])
+    d_s = torch.from_numpy(s.view(np.int32)).to(f"cuda:{local}")
+    d_d = torch.from_numpy(d.view(np.int32)).to(f"cuda:{local}")
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=f"cuda:{local}")
+
+    def run_device():
+        return kc.batch_count(ctx, None, None, off, nn, kk, orientation="degree", autotune=True, use_graph=True,
+                              return_choice=True, return_stats=True, device_ptrs=(d_s.data_ptr(), d_d.data_ptr()))
+
+    def run_host():
+        return kc.batch_count(ctx, s, d, off, nn, kk, orientation="degree", autotune=True, use_graph=True,
+                              return_choice=True, return_stats=True)
+
+    for _ in range(args.warmup):
+        counts, choice, st = run_device()
+    # timed region: inputs (3 GB of edges) are larger than the 126 MB L2
+    barrier(pg, local)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    l0 = L.kc_kernel_launches()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    stage = {"ms_h2d": [], "ms_build": [], "ms_count": []}
+    for i in range(args.steps):
+        evs[i][0].record(stream)
+        counts, choice, st = run_device()
+        evs[i][1].record(stream)
+        for key in stage:
+            stage[key].append(st[key])
+    torch.cuda.synchronize()
+    launches = (L.kc_kernel_launches() - l0) // max(1, args.steps)
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    t_step = max_over_ranks(pg, sum(step_ms) / len(step_ms), local)
+    value = world * G / (t_step / 1e3)
+
+    # end to end through the host API: page-locked inputs, copies inside the step
+    e2e_val = None
+    if not args.no_e2e:
+        counts_h = None
+        barrier(pg, local)
+        ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for i in range(args.steps):
+            ev2[i][0].record(stream)
+            counts_h, _, _ = run_host()
+            ev2[i][1].record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = max_over_ranks(pg, sum(a.elapsed_time(b) for a, b in ev2) / args.steps, local)
+        e2e_val = world * G / (e2e_ms / 1e3)
+        assert counts_h == counts, "host-input and device-input batches disagree"
+
+    total_cliques = sum(counts)
+    out = None
+    if rank == 0:
+        modes = [c["mode"] for c in choice]
+        # plain path: one graph per call on a sample of the same batch
+        P = min(args.plain_sample, G)
+        t0 = time.perf_counter()
+        plain_counts = []
+        for g in range(P):
+            a, b = int(off[g]), int(off[g + 1])
+            with kc.Graph.from_edges(ctx, s[a:b], d[a:b], int(nn[g])) as gr:
+                gr.orient("degree")
+                c = choice[g]
+                plain_counts.append(gr.count(int(kk[g]), mode=c["mode"], unit=c["unit"], part=c["part"],
+                                             encoding=c["encoding"]))
+        t_plain = time.perf_counter() - t0
+        plain_gps = P / t_plain
+        bitexact_plain = plain_counts == counts[:P]
+        cpu = None
+        bitexact_cpu = None
+        if world == 1:
+            from oracle.oracle import max_threads
+
+            done, dt, ccounts = cpu_oracle_sample(s, d, off, nn, kk, modes, args.cpu_seconds)
+            bitexact_cpu = ccounts == counts[:done]
+            cpu = {"value": done / dt, "unit": UNIT, "cores": max_threads(), "kind": "port",
+                   "sample": f"first {done} graphs of the batch, {dt:.1f} s, CPU oracle (OpenMP)",
+                   "bitexact": bitexact_cpu}
+        h2d = 8 * E + 8 * (G + 1) + 8 * G
+        ms_count = sum(stage["ms_count"]) / len(stage["ms_count"])
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64/u128 integer", "data": "synthetic (seeded generators)",
+            "config": {"workload": "batched: %d mixed graphs (ER p~U[.005,.05] / 4-block SBM 0.1,0.005 / ER+planted "
+                                   "clique 20-40), n log-uniform 50-5000, k U{4..12}, degree orientation, autotuned, "
+                                   "one captured counting launch" % G,
+                       "graphs": G, "edges": E, "l2": "inputs (%.1f GB) larger than L2" % (8 * E / 1e9),
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "kcliques_per_s": world * total_cliques / (t_step / 1e3),
+            "plain": {"value": plain_gps, "unit": UNIT, "sample": f"first {P} graphs, one graph per call",
+                      "bitexact": bitexact_plain},
+            "batched_over_plain": value / plain_gps,
+            "stage_ms": {k: sum(v) / len(v) for k, v in stage.items()},
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 16 * G + 24 * G},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "cpu_baseline": cpu,
+            "roofline": None,
+        }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

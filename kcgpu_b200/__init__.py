@@ -1,0 +1,392 @@
+"""kcgpu_b200 — exact k-clique counting on one B200.
+
+Python front end of libkc.so (C ABI: include/kc.h). Every call runs the CUDA
+engine; nothing here computes a count on the CPU.
+
+Mirrors the `-m kc` path of KCGPU:
+  * ``Graph.from_edges`` / ``Graph.from_csr``  ~ EdgeListFile + CSRCOO::from_edgelist
+    (include/FIleReader.cuh:383-411, include/CSRCOO.cuh:37-80), built on the GPU;
+  * ``Graph.orient("degree"|"degen")``         ~ src/main.cu:164-229;
+  * ``Graph.count(k, mode, unit, part, encoding)`` and the
+    ``SingleGPU_Kclique`` class below            ~ kclique/kclique.cuh:1302-2643;
+  * ``parse_spec("o8b")``                       ~ parseKcConfig, include/Config.h:235-271.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import KCError, KcBatchOpts, KcBatchStats, KcCountStats, KcGraphInfo, KcParams, KcU128, check
+
+__all__ = ["Context", "Graph", "KCError", "SingleGPU_Kclique", "parse_spec", "MODES", "UNITS", "ENCODINGS",
+           "ORIENTATIONS", "EdgeList", "gen_er", "gen_rmat", "gen_chung_lu", "gen_sbm", "gen_batch",
+           "batch_count", "footprint_bytes", "lib"]
+
+MODES = {"orient": 0, "orientation": 0, "o": 0, "pivot": 1, "pivoting": 1, "p": 1}
+UNITS = {"node": 0, "edge": 1}
+ENCODINGS = {"bitmap": 0, "binary": 0, "b": 0, "list": 1, "n": 1}
+ORIENTATIONS = {"degree": 0, "degen": 1, "degeneracy": 1}
+
+
+def lib():
+    return _lib.load()
+
+
+def _u32p(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_uint32))
+
+
+def _as_u32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a), dtype=np.uint32)
+
+
+class Context:
+    """One device and one CUDA stream (kc_ctx)."""
+
+    def __init__(self, device: int = 0):
+        L = lib()
+        h = C.c_void_p()
+        check(L.kc_ctx_create(device, C.byref(h)))
+        self._h = h
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def stream_ptr(self) -> int:
+        """The cudaStream_t every call of this context runs on (as an int)."""
+        s = C.c_void_p()
+        check(lib().kc_ctx_get_stream(self._h, C.byref(s)))
+        return int(s.value or 0)
+
+    def close(self):
+        if self._h:
+            lib().kc_ctx_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class CountResult:
+    count: int
+    stats: dict | None = None
+
+
+class Graph:
+    """A device-resident graph (kc_graph)."""
+
+    def __init__(self, ctx: Context, handle):
+        self.ctx = ctx
+        self._h = handle
+
+    @classmethod
+    def from_edges(cls, ctx: Context, src, dst, n_nodes: int = 0) -> "Graph":
+        s, d = _as_u32(src), _as_u32(dst)
+        if s.shape != d.shape:
+            raise ValueError("src and dst must have the same length")
+        h = C.c_void_p()
+        check(lib().kc_graph_from_edges(ctx.handle, _u32p(s), _u32p(d), s.size, n_nodes, C.byref(h)))
+        return cls(ctx, h)
+
+    @classmethod
+    def from_edges_device(cls, ctx: Context, d_src_ptr: int, d_dst_ptr: int, n_edges: int, n_nodes: int = 0):
+        h = C.c_void_p()
+        check(lib().kc_graph_from_edges_device(ctx.handle, C.c_void_p(d_src_ptr), C.c_void_p(d_dst_ptr), n_edges,
+                                               n_nodes, C.byref(h)))
+        return cls(ctx, h)
+
+    @classmethod
+    def from_csr(cls, ctx: Context, row_ptr, col_ind) -> "Graph":
+        rp, ci = _as_u32(row_ptr), _as_u32(col_ind)
+        h = C.c_void_p()
+        check(lib().kc_graph_from_csr(ctx.handle, _u32p(rp), _u32p(ci), rp.size - 1, C.byref(h)))
+        return cls(ctx, h)
+
+    def close(self):
+        if self._h:
+            lib().kc_graph_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> dict:
+        i = KcGraphInfo()
+        check(lib().kc_graph_get_info(self._h, C.byref(i)))
+        return {f: getattr(i, f) for f, _ in KcGraphInfo._fields_}
+
+    @property
+    def n(self) -> int:
+        return self.info()["n"]
+
+    @property
+    def m(self) -> int:
+        return self.info()["m"]
+
+    def csr(self):
+        inf = self.info()
+        rp = np.zeros(inf["n"] + 1, np.uint32)
+        ci = np.zeros(max(1, 2 * inf["m"]), np.uint32)
+        check(lib().kc_graph_get_csr(self._h, _u32p(rp), _u32p(ci)))
+        return rp, ci[: 2 * inf["m"]]
+
+    def orient(self, orientation="degree") -> "Graph":
+        o = ORIENTATIONS[orientation] if isinstance(orientation, str) else int(orientation)
+        check(lib().kc_orient(self._h, o))
+        return self
+
+    def dag(self):
+        inf = self.info()
+        rp = np.zeros(inf["n"] + 1, np.uint32)
+        ci = np.zeros(max(1, inf["m"]), np.uint32)
+        check(lib().kc_graph_get_dag(self._h, _u32p(rp), _u32p(ci)))
+        return rp, ci[: inf["m"]]
+
+    def peel(self):
+        n = self.info()["n"]
+        prio = np.zeros(max(1, n), np.uint32)
+        lev = np.zeros(max(1, n), np.uint32)
+        check(lib().kc_graph_get_peel(self._h, _u32p(prio), _u32p(lev)))
+        return prio[:n], lev[:n]
+
+    def count(self, k: int, mode="orient", unit="node", part: int = 8, encoding="bitmap",
+              stats: bool = False):
+        """Exact number of k-cliques (a Python int; 128-bit on the device)."""
+        p = KcParams()
+        p.k = k
+        p.mode = MODES[mode] if isinstance(mode, str) else int(mode)
+        p.unit = UNITS[unit] if isinstance(unit, str) else int(unit)
+        p.part = part
+        p.encoding = ENCODINGS[encoding] if isinstance(encoding, str) else int(encoding)
+        p.flags = 1 if stats else 0
+        out = KcU128()
+        st = KcCountStats()
+        check(lib().kc_count(self._h, C.byref(p), C.byref(out), C.byref(st)))
+        if stats:
+            return CountResult(out.value(), {f: getattr(st, f) for f, _ in KcCountStats._fields_})
+        return out.value()
+
+    def kcore(self):
+        n = self.info()["n"]
+        core = np.zeros(max(1, n), np.uint32)
+        mx = C.c_uint32()
+        check(lib().kc_kcore(self._h, _u32p(core), C.byref(mx)))
+        return core[:n], int(mx.value)
+
+    def truss_support(self) -> np.ndarray:
+        m = self.info()["m"]
+        sup = np.zeros(max(1, m), np.uint32)
+        check(lib().kc_truss_support(self._h, _u32p(sup)))
+        return sup[:m]
+
+
+def parse_spec(spec: str) -> dict:
+    """The reference's -q grammar: [o|p]<part>[b|n|h] (include/Config.h:235-271)."""
+    p = KcParams()
+    check(lib().kc_parse_spec(spec.encode() if spec is not None else None, C.byref(p)))
+    return {"mode": int(p.mode), "part": int(p.part), "encoding": int(p.encoding)}
+
+
+class SingleGPU_Kclique:
+    """Mirror of graph::SingleGPU_Kclique<uint> (kclique/kclique.cuh:1302-2643).
+
+    The reference's methods print the count per degree window and return the
+    window level from count(); here each method returns the exact k-clique count
+    and count() returns the last one.
+    """
+
+    def __init__(self, dev: int, g: Graph):
+        self.dev = dev
+        self.g = g
+        self._last = None
+
+    def _run(self, k, unit, mode, enc, part):
+        self._last = self.g.count(k, mode=mode, unit=unit, part=part, encoding=enc)
+        return self._last
+
+    def findKclqueIncremental_node_async(self, k, part=8):
+        return self._run(k, "node", "orient", "list", part)
+
+    def findKclqueIncremental_node_binary_async(self, k, part=8):
+        return self._run(k, "node", "orient", "bitmap", part)
+
+    def findKclqueIncremental_node_pivot_async(self, k, part=8):
+        return self._run(k, "node", "pivot", "bitmap", part)
+
+    def findKclqueIncremental_node_nobin_pivot_async(self, k, part=8):
+        return self._run(k, "node", "pivot", "list", part)
+
+    def findKclqueIncremental_edge_async(self, k, part=8):
+        return self._run(k, "edge", "orient", "list", part)
+
+    def findKclqueIncremental_edge_binary_async(self, k, part=8):
+        return self._run(k, "edge", "orient", "bitmap", part)
+
+    def findKclqueIncremental_edge_pivot_async(self, k, part=8):
+        return self._run(k, "edge", "pivot", "bitmap", part)
+
+    def findKclqueIncremental_edge_nobin_pivot_async(self, k, part=8):
+        return self._run(k, "edge", "pivot", "list", part)
+
+    def sync(self):
+        return None
+
+    def count(self):
+        return self._last
+
+
+# ---- synthetic inputs ---------------------------------------------------------
+
+class EdgeList:
+    """A host edge list owned by the library (optionally page-locked)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    def arrays(self, copy: bool = True):
+        s = C.POINTER(C.c_uint32)()
+        d = C.POINTER(C.c_uint32)()
+        ne = C.c_uint64()
+        nn = C.c_uint32()
+        check(lib().kc_edgelist_data(self._h, C.byref(s), C.byref(d), C.byref(ne), C.byref(nn)))
+        n = int(ne.value)
+        if n == 0:
+            return np.zeros(0, np.uint32), np.zeros(0, np.uint32), int(nn.value)
+        a = np.ctypeslib.as_array(s, shape=(n,))
+        b = np.ctypeslib.as_array(d, shape=(n,))
+        if copy:
+            a, b = a.copy(), b.copy()
+        return a, b, int(nn.value)
+
+    def pointers(self):
+        s = C.POINTER(C.c_uint32)()
+        d = C.POINTER(C.c_uint32)()
+        ne = C.c_uint64()
+        nn = C.c_uint32()
+        check(lib().kc_edgelist_data(self._h, C.byref(s), C.byref(d), C.byref(ne), C.byref(nn)))
+        return s, d, int(ne.value), int(nn.value)
+
+    def plant_cliques(self, count: int, smin: int, smax: int, seed: int):
+        check(lib().kc_gen_plant_cliques(self._h, count, smin, smax, seed))
+        return self
+
+    def batch_meta(self):
+        off = C.POINTER(C.c_uint64)()
+        nn = C.POINTER(C.c_uint32)()
+        kk = C.POINTER(C.c_uint32)()
+        fam = C.POINTER(C.c_uint32)()
+        ng = C.c_uint32()
+        check(lib().kc_batchgen_meta(self._h, C.byref(off), C.byref(nn), C.byref(kk), C.byref(fam), C.byref(ng)))
+        g = int(ng.value)
+        return (np.ctypeslib.as_array(off, shape=(g + 1,)).copy(), np.ctypeslib.as_array(nn, shape=(g,)).copy(),
+                np.ctypeslib.as_array(kk, shape=(g,)).copy(), np.ctypeslib.as_array(fam, shape=(g,)).copy())
+
+    def close(self):
+        if self._h:
+            lib().kc_edgelist_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _gen(fn, *args) -> EdgeList:
+    h = C.c_void_p()
+    check(fn(*args, C.byref(h)))
+    return EdgeList(h)
+
+
+def gen_er(n: int, p: float, seed: int, pinned: bool = False) -> EdgeList:
+    return _gen(lib().kc_gen_er, n, p, seed, int(pinned))
+
+
+def gen_rmat(scale: int, edge_factor: float, a=0.57, b=0.19, c=0.19, seed: int = 1, pinned: bool = False) -> EdgeList:
+    return _gen(lib().kc_gen_rmat, scale, edge_factor, a, b, c, seed, int(pinned))
+
+
+def gen_chung_lu(n: int, exponent: float, mean_degree: float, max_degree: float, seed: int,
+                 pinned: bool = False) -> EdgeList:
+    return _gen(lib().kc_gen_chung_lu, n, exponent, mean_degree, max_degree, seed, int(pinned))
+
+
+def gen_sbm(n: int, blocks: int, p_in: float, p_out: float, seed: int, pinned: bool = False) -> EdgeList:
+    return _gen(lib().kc_gen_sbm, n, blocks, p_in, p_out, seed, int(pinned))
+
+
+def gen_batch(n_graphs: int, base_seed: int, n_min=50, n_max=5000, k_min=4, k_max=12, pinned=False) -> EdgeList:
+    return _gen(lib().kc_gen_batch, n_graphs, base_seed, n_min, n_max, k_min, k_max, int(pinned))
+
+
+def footprint_bytes(n_nodes: int, n_edges: int, max_out: int) -> int:
+    return int(lib().kc_footprint_bytes(n_nodes, n_edges, max_out))
+
+
+def batch_count(ctx: Context, src, dst, edge_off, n_nodes, ks, orientation="degree", autotune=True,
+                fixed: dict | None = None, use_graph=True, return_choice=False, return_stats=False,
+                device_ptrs: tuple | None = None):
+    """Counts a packed batch: graph i owns edges [edge_off[i], edge_off[i+1]).
+
+    With device_ptrs=(d_src, d_dst) the edges are read from device memory of
+    the context's GPU (src/dst are then ignored)."""
+    if device_ptrs is None:
+        s, d = _as_u32(src), _as_u32(dst)
+    off = np.ascontiguousarray(edge_off, dtype=np.uint64)
+    nn = _as_u32(n_nodes)
+    kk = _as_u32(ks)
+    g = nn.size
+    opts = KcBatchOpts()
+    opts.orientation = ORIENTATIONS[orientation] if isinstance(orientation, str) else int(orientation)
+    opts.autotune = 1 if autotune else 0
+    opts.use_graph = 1 if use_graph else 0
+    if fixed:
+        opts.fixed.mode = MODES.get(fixed.get("mode", "orient"), 0) if isinstance(fixed.get("mode"), str) else int(fixed.get("mode", 0))
+        opts.fixed.unit = UNITS.get(fixed.get("unit", "node"), 0) if isinstance(fixed.get("unit"), str) else int(fixed.get("unit", 0))
+        opts.fixed.part = int(fixed.get("part", 8))
+        opts.fixed.encoding = ENCODINGS.get(fixed.get("encoding", "bitmap"), 0) if isinstance(fixed.get("encoding"), str) else int(fixed.get("encoding", 0))
+    counts = (KcU128 * g)()
+    choice = (KcParams * g)()
+    st = KcBatchStats()
+    offp = off.ctypes.data_as(C.POINTER(C.c_uint64))
+    if device_ptrs is None:
+        check(lib().kc_batch_count_packed(ctx.handle, _u32p(s), _u32p(d), offp, _u32p(nn), _u32p(kk), g,
+                                          C.byref(opts), counts, choice, C.byref(st)))
+    else:
+        check(lib().kc_batch_count_packed_device(ctx.handle, C.c_void_p(device_ptrs[0]), C.c_void_p(device_ptrs[1]),
+                                                 offp, _u32p(nn), _u32p(kk), g, C.byref(opts), counts, choice,
+                                                 C.byref(st)))
+    res = [c.value() for c in counts]
+    out = [res]
+    if return_choice:
+        out.append([{"mode": int(c.mode), "unit": int(c.unit), "part": int(c.part), "encoding": int(c.encoding)}
+                    for c in choice])
+    if return_stats:
+        out.append({f: getattr(st, f) for f, _ in KcBatchStats._fields_})
+    return out[0] if len(out) == 1 else tuple(out)

@@ -1,0 +1,384 @@
+// Batched counting: thousands of small graphs in one pass.
+//
+// No counterpart in the reference (one graph per process there). The batch is
+// treated as ONE disjoint-union graph: ids of graph i are shifted by the
+// vertex count of the graphs before it, so CSR build, orientation and the
+// counting queue run once over the whole batch instead of once per graph.
+// This is exact for both orientations: degree order only compares vertices
+// of the same graph, and the degeneracy peel of a disjoint union visits each
+// graph's (level, sub-round) pairs in the same order as a peel of that graph
+// alone, so every graph keeps its own relative priority order (the union's
+// final batch and a lone graph's final batch both get the largest priority).
+//
+// Every vertex carries its graph id; every unit reads the k of its graph and
+// adds its count to its graph's 128-bit slot. The autotuner picks mode, unit,
+// partition size and encoding per graph from its shape; graphs that share a
+// choice form one counting pass, and all passes of the batch are captured into
+// one CUDA graph that is launched once.
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <tuple>
+#include <vector>
+
+#include "count_kernels.cuh"
+#include "dev_common.cuh"
+#include "engine.h"
+#include "prims.cuh"
+
+namespace kc {
+
+namespace {
+
+__global__ void k_globalize(uint32_t* src, uint32_t* dst, const unsigned long long* __restrict__ eoff,
+                            const uint32_t* __restrict__ voff, const uint32_t* __restrict__ nn, uint32_t G,
+                            uint32_t* err) {
+  for (uint32_t g = blockIdx.x; g < G; g += gridDim.x) {
+    const unsigned long long b = eoff[g], e = eoff[g + 1];
+    const uint32_t off = voff[g], n = nn[g];
+    for (unsigned long long i = b + threadIdx.x; i < e; i += blockDim.x) {
+      uint32_t u = src[i], v = dst[i];
+      if (u >= n || v >= n) {
+        atomicCAS(err, 0u, g + 1u);
+        u = v = 0;
+      }
+      src[i] = u + off;
+      dst[i] = v + off;
+    }
+  }
+}
+
+__global__ void k_vertex_graph(const uint32_t* __restrict__ voff, uint32_t G, uint32_t* vg) {
+  for (uint32_t g = blockIdx.x; g < G; g += gridDim.x)
+    for (uint32_t v = voff[g] + threadIdx.x; v < voff[g + 1]; v += blockDim.x) vg[v] = g;
+}
+
+__global__ void k_rank_graph(const uint32_t* __restrict__ vg_orig, const uint32_t* __restrict__ rank, uint32_t n,
+                             uint32_t* vgraph) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    vgraph[rank[v]] = vg_orig[v];
+}
+
+// Per graph: largest out-degree, edge count and largest peel level.
+__global__ void k_graph_features(const uint32_t* __restrict__ drp, const uint32_t* __restrict__ vgraph,
+                                 const uint32_t* __restrict__ inv, const uint32_t* __restrict__ level, uint32_t n,
+                                 uint32_t* fmax, unsigned long long* fm, uint32_t* fcore) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const uint32_t g = vgraph[r];
+    const uint32_t d = drp[r + 1] - drp[r];
+    atomicMax(&fmax[g], d);
+    if (d) atomicAdd(&fm[g], (unsigned long long)d);
+    if (level) atomicMax(&fcore[g], level[inv[r]]);
+  }
+}
+
+uint32_t grid_for(uint64_t work, int sms) {
+  return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((work + 255) / 256, (uint64_t)sms * 16));
+}
+
+void free_union(kc_graph* g) {
+  void* ps[] = {g->rp, g->col, g->rank, g->inv, g->drp, g->dcol, g->erow, g->prio, g->level, g->vgraph};
+  for (void* p : ps)
+    if (p) cudaFreeAsync(p, g->ctx->stream);
+}
+
+struct Choice {
+  uint32_t mode, unit, part, enc;
+  bool operator<(const Choice& o) const {
+    return std::tie(mode, unit, part, enc) < std::tie(o.mode, o.unit, o.part, o.enc);
+  }
+};
+
+kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool device_input,
+                    const uint64_t* edge_off, const uint32_t* n_nodes, const uint32_t* ks, uint32_t G,
+                    const kc_batch_opts* opts, kc_u128* counts, kc_params* choice, kc_batch_stats* stats) {
+  const double t0 = now_ms();
+  cudaStream_t s = ctx->stream;
+  if (G == 0) return KC_OK;
+  if (!src || !dst || !edge_off || !n_nodes || !ks || !counts)
+    return fail(KC_ERR_INVALID_ARG, "NULL argument");
+  if (opts && opts->orientation > KC_ORIENT_DEGEN) return fail(KC_ERR_INVALID_ARG, "unknown orientation");
+  std::vector<uint32_t> voff((size_t)G + 1, 0);
+  uint64_t N = 0;
+  for (uint32_t g = 0; g < G; ++g) {
+    if (ks[g] < 1) return fail(KC_ERR_INVALID_ARG, "graph %u: k must be >= 1", g);
+    if (edge_off[g + 1] < edge_off[g]) return fail(KC_ERR_INVALID_ARG, "edge_off decreases at graph %u", g);
+    voff[g] = (uint32_t)N;
+    N += n_nodes[g];
+    if (N >= 0xffffffffull) return fail(KC_ERR_INVALID_ARG, "the batch holds more than 2^32-2 vertices");
+  }
+  voff[G] = (uint32_t)N;
+  const uint64_t E = edge_off[G] - edge_off[0];
+  const uint32_t orientation = opts ? opts->orientation : KC_ORIENT_DEGREE;
+
+  cudaEvent_t e0, e1, e2, e3, e4;
+  cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2); cudaEventCreate(&e3); cudaEventCreate(&e4);
+  uint32_t *ds = nullptr, *dd = nullptr, *dvoff = nullptr, *dnn = nullptr, *derr = nullptr, *vg = nullptr;
+  unsigned long long* deoff = nullptr;
+  KC_CUDA(cudaMallocAsync(&ds, sizeof(uint32_t) * std::max<uint64_t>(1, E), s));
+  KC_CUDA(cudaMallocAsync(&dd, sizeof(uint32_t) * std::max<uint64_t>(1, E), s));
+  KC_CUDA(cudaMallocAsync(&deoff, sizeof(unsigned long long) * ((size_t)G + 1), s));
+  KC_CUDA(cudaMallocAsync(&dvoff, sizeof(uint32_t) * ((size_t)G + 1), s));
+  KC_CUDA(cudaMallocAsync(&dnn, sizeof(uint32_t) * G, s));
+  KC_CUDA(cudaMallocAsync(&derr, sizeof(uint32_t) * 4, s));
+  KC_CUDA(cudaMemsetAsync(derr, 0, sizeof(uint32_t) * 4, s));
+  std::vector<unsigned long long> eoff_rel((size_t)G + 1);
+  for (uint32_t g = 0; g <= G; ++g) eoff_rel[g] = edge_off[g] - edge_off[0];
+  cudaEventRecord(e0, s);
+  if (E) {
+    const cudaMemcpyKind kind = device_input ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    KC_CUDA(cudaMemcpyAsync(ds, src + edge_off[0], sizeof(uint32_t) * E, kind, s));
+    KC_CUDA(cudaMemcpyAsync(dd, dst + edge_off[0], sizeof(uint32_t) * E, kind, s));
+  }
+  KC_CUDA(cudaMemcpyAsync(deoff, eoff_rel.data(), sizeof(unsigned long long) * ((size_t)G + 1), cudaMemcpyHostToDevice, s));
+  KC_CUDA(cudaMemcpyAsync(dvoff, voff.data(), sizeof(uint32_t) * ((size_t)G + 1), cudaMemcpyHostToDevice, s));
+  KC_CUDA(cudaMemcpyAsync(dnn, n_nodes, sizeof(uint32_t) * G, cudaMemcpyHostToDevice, s));
+  cudaEventRecord(e1, s);
+  k_globalize<<<std::min<uint32_t>(G, 65535), 256, 0, s>>>(ds, dd, deoff, dvoff, dnn, G, derr);
+  uint32_t herr = 0;
+  KC_CUDA(cudaMemcpyAsync(&herr, derr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  KC_CUDA(cudaStreamSynchronize(s));
+  if (herr) return fail(KC_ERR_INVALID_ARG, "graph %u has an endpoint not below its n_nodes", herr - 1);
+
+  kc_graph U;
+  U.ctx = ctx;
+  kc_status st = build_csr(&U, ds, dd, E, (uint32_t)N);
+  cudaFreeAsync(ds, s);
+  cudaFreeAsync(dd, s);
+  if (st == KC_OK) st = orient_graph(&U, orientation);
+  if (st == KC_OK) {
+    KC_CUDA(cudaMallocAsync(&vg, sizeof(uint32_t) * std::max<uint64_t>(1, N), s));
+    st = dev_alloc(&U, (void**)&U.vgraph, sizeof(uint32_t) * std::max<uint64_t>(1, N));
+  }
+  std::vector<uint32_t> fmax(G, 0), fcore(G, 0);
+  std::vector<unsigned long long> fm(G, 0);
+  if (st == KC_OK) {
+    k_vertex_graph<<<std::min<uint32_t>(G, 65535), 256, 0, s>>>(dvoff, G, vg);
+    k_rank_graph<<<grid_for(N, ctx->sms), 256, 0, s>>>(vg, U.rank, (uint32_t)N, U.vgraph);
+    uint32_t *dfmax = nullptr, *dfcore = nullptr;
+    unsigned long long* dfm = nullptr;
+    KC_CUDA(cudaMallocAsync(&dfmax, sizeof(uint32_t) * G, s));
+    KC_CUDA(cudaMallocAsync(&dfcore, sizeof(uint32_t) * G, s));
+    KC_CUDA(cudaMallocAsync(&dfm, sizeof(unsigned long long) * G, s));
+    KC_CUDA(cudaMemsetAsync(dfmax, 0, sizeof(uint32_t) * G, s));
+    KC_CUDA(cudaMemsetAsync(dfcore, 0, sizeof(uint32_t) * G, s));
+    KC_CUDA(cudaMemsetAsync(dfm, 0, sizeof(unsigned long long) * G, s));
+    k_graph_features<<<grid_for(N, ctx->sms), 256, 0, s>>>(U.drp, U.vgraph, U.inv, U.level, (uint32_t)N, dfmax, dfm,
+                                                          dfcore);
+    KC_CUDA(cudaMemcpyAsync(fmax.data(), dfmax, sizeof(uint32_t) * G, cudaMemcpyDeviceToHost, s));
+    KC_CUDA(cudaMemcpyAsync(fcore.data(), dfcore, sizeof(uint32_t) * G, cudaMemcpyDeviceToHost, s));
+    KC_CUDA(cudaMemcpyAsync(fm.data(), dfm, sizeof(unsigned long long) * G, cudaMemcpyDeviceToHost, s));
+    cudaEventRecord(e2, s);
+    KC_CUDA(cudaStreamSynchronize(s));
+    cudaFreeAsync(dfmax, s);
+    cudaFreeAsync(dfcore, s);
+    cudaFreeAsync(dfm, s);
+  }
+  if (vg) cudaFreeAsync(vg, s);
+
+  // per-graph choices, grouped into counting passes
+  std::map<Choice, std::vector<uint32_t>> groups;
+  std::vector<kc_params> picked(G);
+  if (st == KC_OK) {
+    for (uint32_t g = 0; g < G; ++g) {
+      kc_params p;
+      if (!opts || opts->autotune) {
+        p = autotune(n_nodes[g], fm[g], fmax[g], ks[g], fcore[g]);
+      } else {
+        p = opts->fixed;
+        if (p.part == 0) p.part = 8;
+      }
+      p.k = ks[g];
+      if (ks[g] <= 2) p.unit = KC_UNIT_NODE;  // an edge unit cannot count 1-cliques
+      p.flags = 0;
+      if (p.mode > 1 || p.unit > 1 || p.encoding > 1 || p.part == 0 || p.part > 32 || (p.part & (p.part - 1))) {
+        st = fail(KC_ERR_INVALID_ARG, "bad fixed parameters for the batch");
+        break;
+      }
+      picked[g] = p;
+      groups[Choice{p.mode, p.unit, p.part, p.encoding}].push_back(g);
+    }
+  }
+
+  unsigned long long* dout = nullptr;
+  std::vector<uint32_t*> gks;
+  std::vector<CountPlan> plans;
+  cudaGraph_t cg = nullptr;
+  cudaGraphExec_t cge = nullptr;
+  uint32_t kernels = 0;
+  uint64_t units = 0;
+  if (st == KC_OK) {
+    KC_CUDA(cudaMallocAsync(&dout, sizeof(unsigned long long) * 2 * G, s));
+    plans.reserve(groups.size());
+    for (auto& kv : groups) {
+      std::vector<uint32_t> hk(G, 0xffffffffu);
+      uint32_t kmax = 0;
+      for (uint32_t g : kv.second) {
+        hk[g] = ks[g];
+        kmax = std::max(kmax, ks[g]);
+      }
+      uint32_t* dk = nullptr;
+      KC_CUDA(cudaMallocAsync(&dk, sizeof(uint32_t) * G, s));
+      KC_CUDA(cudaMemcpyAsync(dk, hk.data(), sizeof(uint32_t) * G, cudaMemcpyHostToDevice, s));
+      gks.push_back(dk);
+      CountRequest req;
+      req.k = kmax;
+      req.mode = kv.first.mode;
+      req.unit = kv.first.unit;
+      req.part = kv.first.part;
+      req.encoding = kv.first.enc;
+      req.flags = 0;
+      req.d_graph_k = dk;
+      req.n_graphs = G;
+      req.k_max = kmax;
+      plans.emplace_back();
+      st = count_prepare(&U, req, dout, 0, &plans.back());
+      if (st != KC_OK) break;
+    }
+  }
+  if (st == KC_OK) {
+    KC_CUDA(cudaMemsetAsync(dout, 0, sizeof(unsigned long long) * 2 * G, s));
+    KC_CUDA(cudaStreamSynchronize(s));
+    const bool use_graph = !opts || opts->use_graph;
+    if (use_graph) {
+      KC_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      for (auto& pl : plans) {
+        st = count_enqueue(pl, s);
+        if (st != KC_OK) break;
+      }
+      cudaError_t ce = cudaStreamEndCapture(s, &cg);
+      if (st == KC_OK && ce != cudaSuccess) st = cuda_fail(ce, "cudaStreamEndCapture", __FILE__, __LINE__);
+      if (st == KC_OK) {
+        ce = cudaGraphInstantiate(&cge, cg, 0);
+        if (ce != cudaSuccess) st = cuda_fail(ce, "cudaGraphInstantiate", __FILE__, __LINE__);
+      }
+      if (st == KC_OK) {
+        cudaEventRecord(e3, s);
+        ce = cudaGraphLaunch(cge, s);
+        cudaEventRecord(e4, s);
+        if (ce != cudaSuccess) st = cuda_fail(ce, "cudaGraphLaunch", __FILE__, __LINE__);
+      }
+    } else {
+      cudaEventRecord(e3, s);
+      for (auto& pl : plans) {
+        st = count_enqueue(pl, s);
+        if (st != KC_OK) break;
+      }
+      cudaEventRecord(e4, s);
+    }
+  }
+  if (st == KC_OK) {
+    bool deep = false;
+    for (auto& pl : plans) {
+      uint32_t err = count_error(pl, s, nullptr);
+      if (err == DEV_ERR_STACK) deep = true;
+      else if (err) st = fail(KC_ERR_INTERNAL, "batched counting reported device error %u", err);
+      units += count_units(pl, s);
+      kernels += 5;
+      for (int c = 0; c < kNumClasses; ++c) kernels += pl.active[c] ? 1 : 0;
+    }
+    if (st == KC_OK && deep) {
+      // a clique tree deeper than the fast stack: rerun every pass with full depth
+      KC_CUDA(cudaMemsetAsync(dout, 0, sizeof(unsigned long long) * 2 * G, s));
+      for (size_t i = 0; i < plans.size() && st == KC_OK; ++i) {
+        CountRequest req = plans[i].req;
+        count_release(&plans[i]);
+        plans[i] = CountPlan();
+        st = count_prepare(&U, req, dout, 1, &plans[i]);
+        if (st == KC_OK) st = count_enqueue(plans[i], s);
+        if (st == KC_OK) {
+          uint32_t err = count_error(plans[i], s, nullptr);
+          if (err) st = fail(KC_ERR_INTERNAL, "batched counting reported device error %u", err);
+        }
+      }
+    }
+  }
+  std::vector<unsigned long long> hout(2 * (size_t)G, 0);
+  if (st == KC_OK) {
+    KC_CUDA(cudaMemcpyAsync(hout.data(), dout, sizeof(unsigned long long) * 2 * G, cudaMemcpyDeviceToHost, s));
+    KC_CUDA(cudaStreamSynchronize(s));
+    for (uint32_t g = 0; g < G; ++g) {
+      counts[g].lo = hout[2 * g];
+      counts[g].hi = hout[2 * g + 1];
+      if (choice) choice[g] = picked[g];
+    }
+  }
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    float a = 0, b = 0, c = 0;
+    cudaEventElapsedTime(&a, e0, e1);
+    cudaEventElapsedTime(&b, e1, e2);
+    cudaEventElapsedTime(&c, e3, e4);
+    stats->ms_h2d = a;
+    stats->ms_build = b;
+    stats->ms_count = c;
+    stats->units = units;
+    stats->kernels = kernels;
+    stats->n_graphs = G;
+  }
+  if (cge) cudaGraphExecDestroy(cge);
+  if (cg) cudaGraphDestroy(cg);
+  for (auto& pl : plans) count_release(&pl);
+  for (auto* p : gks) cudaFreeAsync(p, s);
+  if (dout) cudaFreeAsync(dout, s);
+  cudaFreeAsync(deoff, s);
+  cudaFreeAsync(dvoff, s);
+  cudaFreeAsync(dnn, s);
+  cudaFreeAsync(derr, s);
+  free_union(&U);
+  cudaStreamSynchronize(s);
+  cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2); cudaEventDestroy(e3); cudaEventDestroy(e4);
+  if (stats) stats->ms_total = now_ms() - t0;
+  return st;
+}
+
+}  // namespace
+}  // namespace kc
+
+extern "C" {
+
+kc_status kc_batch_count_packed(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, const uint64_t* edge_off,
+                                const uint32_t* n_nodes, const uint32_t* k, uint32_t n_graphs,
+                                const kc_batch_opts* opts, kc_u128* counts, kc_params* choice,
+                                kc_batch_stats* stats) {
+  if (!ctx) return kc::fail(KC_ERR_INVALID_ARG, "context is NULL");
+  std::lock_guard<std::mutex> l(ctx->mu);
+  cudaSetDevice(ctx->device);
+  kc::clear_error();
+  return kc::run_batch(ctx, src, dst, false, edge_off, n_nodes, k, n_graphs, opts, counts, choice, stats);
+}
+
+kc_status kc_batch_count_packed_device(kc_ctx* ctx, const uint32_t* d_src, const uint32_t* d_dst,
+                                       const uint64_t* edge_off, const uint32_t* n_nodes, const uint32_t* k,
+                                       uint32_t n_graphs, const kc_batch_opts* opts, kc_u128* counts,
+                                       kc_params* choice, kc_batch_stats* stats) {
+  if (!ctx) return kc::fail(KC_ERR_INVALID_ARG, "context is NULL");
+  std::lock_guard<std::mutex> l(ctx->mu);
+  cudaSetDevice(ctx->device);
+  kc::clear_error();
+  return kc::run_batch(ctx, d_src, d_dst, true, edge_off, n_nodes, k, n_graphs, opts, counts, choice, stats);
+}
+
+kc_status kc_batch_count(kc_ctx* ctx, const kc_batch_graph* graphs, uint32_t n_graphs, const kc_batch_opts* opts,
+                         kc_u128* counts, kc_params* choice, kc_batch_stats* stats) {
+  if (!ctx || (n_graphs && !graphs)) return kc::fail(KC_ERR_INVALID_ARG, "NULL argument");
+  std::vector<uint64_t> off((size_t)n_graphs + 1, 0);
+  for (uint32_t g = 0; g < n_graphs; ++g) {
+    if (graphs[g].n_edges && (!graphs[g].src || !graphs[g].dst))
+      return kc::fail(KC_ERR_INVALID_ARG, "graph %u: edge arrays are NULL", g);
+    off[g + 1] = off[g] + graphs[g].n_edges;
+  }
+  std::vector<uint32_t> s(off[n_graphs]), d(off[n_graphs]), nn(n_graphs), kk(n_graphs);
+  for (uint32_t g = 0; g < n_graphs; ++g) {
+    if (graphs[g].n_edges) {
+      std::memcpy(s.data() + off[g], graphs[g].src, sizeof(uint32_t) * graphs[g].n_edges);
+      std::memcpy(d.data() + off[g], graphs[g].dst, sizeof(uint32_t) * graphs[g].n_edges);
+    }
+    nn[g] = graphs[g].n_nodes;
+    kk[g] = graphs[g].k;
+  }
+  return kc_batch_count_packed(ctx, s.data(), d.data(), off.data(), nn.data(), kk.data(), n_graphs, opts, counts,
+                               choice, stats);
+}
+
+}  // extern "C"

@@ -1,0 +1,302 @@
+// k-clique counting: the unit queue and the per-class persistent launches.
+//
+// Reference kernels replaced (kclique/):
+//   node / orientation / bitmap  kckernel_node_block_warp_binary_count       kckernels_orientation.cuh:319-475
+//   edge / orientation / bitmap  kckernel_edge_block_warp_binary_count_o2    kckernels_orientation.cuh:479-650
+//   node / pivot / bitmap        kckernel_node_block_warp_binary_pivot_count kckernels_pivoting.cuh:2-346
+//   edge / pivot / bitmap        kckernel_edge_block_warp_binary_pivot_count kckernels.cuh:2263-2630
+//   and the list-encoded variants (count_list.cu).
+//
+// Unit semantics (as the reference): a node unit u counts the k-cliques whose
+// lowest-ranked vertex is u, i.e. the (k-1)-cliques of the DAG induced on
+// S = N+(u); an edge unit u->v counts those whose two lowest are u and v, the
+// (k-2)-cliques on S = N+(u) ∩ N+(v). Units that cannot hold a k-clique
+// (|N+(u)| < k-1, or min(|N+(u)|, |N+(v)|) < k-2) are dropped up front, as
+// the reference's first bucket_scan does (kclique.cuh:1610-1614, 2041).
+//
+// The persistent work queue replaces GraphQueue + bucket_scan
+// (include/GraphQueue.cuh, kclique.cuh:1318-1406): units are sorted by
+// decreasing size with a counting sort, split into size classes whose bounds
+// are computed on the device, and each class runs one persistent grid that
+// takes units from a global ticket — heavy units first, no per-window launch
+// or host synchronisation (kclique.cuh:1645-1675 launches per 1024-wide
+// degree window and syncs the host after each).
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "count_kernels.cuh"
+#include "dev_common.cuh"
+#include "engine.h"
+#include "prims.cuh"
+
+namespace kc {
+
+namespace {
+
+__global__ void k_unit_sizes(const uint32_t* __restrict__ drp, const uint32_t* __restrict__ dcol,
+                             const uint32_t* __restrict__ erow, uint32_t n_units, int edge,
+                             const uint32_t* __restrict__ vgraph, const uint32_t* __restrict__ gk, uint32_t k0,
+                             uint32_t* size, uint32_t* hist) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_units; i += gridDim.x * blockDim.x) {
+    uint32_t s, src;
+    if (!edge) {
+      src = i;
+      s = drp[i + 1] - drp[i];
+    } else {
+      src = erow[i];
+      const uint32_t v = dcol[i];
+      s = min(drp[src + 1] - drp[src], drp[v + 1] - drp[v]);
+    }
+    const uint32_t k = gk ? gk[vgraph ? vgraph[src] : 0u] : k0;
+    bool keep;
+    if (k == 0xffffffffu || k == 0u) keep = false;  // graph not in this pass
+    else if (edge) keep = k >= 2u && s >= k - 2u;
+    else keep = s >= k - 1u;
+    size[i] = keep ? s : 0xffffffffu;
+    if (keep) atomicAdd(&hist[s], 1u);
+  }
+}
+
+__global__ void k_reverse(const uint32_t* __restrict__ in, uint32_t n, uint32_t* out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = in[n - 1 - i];
+}
+
+struct ClassSpec {
+  int64_t lo, hi;   // unit sizes (lo, hi]
+  uint32_t G;       // threads per unit group
+  uint32_t block;   // threads per CTA
+};
+
+// Size classes, largest first (the queue is sorted by decreasing size).
+const ClassSpec kClasses[kNumClasses] = {
+    {1024, 0xffffffffll, 256, 256},  // CTA per unit, bitmap in global memory
+    {128, 1024, 256, 256},           // CTA per unit, bitmap in shared memory
+    {32, 128, 32, 128},              // warp per unit
+    {-1, 32, 32, 128},               // warp per unit, one word per row
+};
+
+// Class c holds the units of sizes (lo, hi], i.e. reversed indices
+// [max-hi, max-lo) of the descending order; scan = exclusive scan of the
+// reversed histogram (max + 2 entries).
+__global__ void k_class_bounds(const uint32_t* __restrict__ scan, uint32_t max_size, uint32_t* bounds) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int64_t M = max_size;
+  const int64_t lo[kNumClasses] = {1024, 128, 32, -1};
+  const int64_t hi[kNumClasses] = {0xffffffffll, 1024, 128, 32};
+  for (int c = 0; c < kNumClasses; ++c) {
+    uint32_t b = 0, e = 0;
+    if (M > lo[c]) {
+      const int64_t h = hi[c] < M ? hi[c] : M;
+      b = scan[M - h];
+      e = scan[M - lo[c]];
+    }
+    bounds[2 * c] = b;
+    bounds[2 * c + 1] = e - b;
+  }
+}
+
+__global__ void k_unit_scatter(const uint32_t* __restrict__ size, uint32_t n_units, uint32_t max_size,
+                               uint32_t* cursor, uint32_t* queue) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_units; i += gridDim.x * blockDim.x) {
+    const uint32_t s = size[i];
+    if (s == 0xffffffffu) continue;
+    queue[atomicAdd(&cursor[max_size - s], 1u)] = i;
+  }
+}
+
+uint32_t auto_part(uint32_t mode, uint32_t W) {
+  if (mode == KC_MODE_ORIENT) return W <= 1 ? 1u : (W <= 2 ? 2u : (W <= 4 ? 4u : (W <= 8 ? 8u : (W <= 16 ? 16u : 32u))));
+  return W <= 2 ? 4u : (W <= 4 ? 8u : (W <= 8 ? 16u : 32u));
+}
+
+}  // namespace
+
+kc_status ensure_binom(kc_ctx* ctx, uint32_t rows, uint32_t cols) {
+  if (ctx->d_binom && ctx->brows >= rows && ctx->bcols >= cols) return KC_OK;
+  rows = std::max(rows, ctx->brows);
+  cols = std::max(cols, ctx->bcols);
+  std::vector<unsigned __int128> t((size_t)(rows + 1) * (cols + 1), 0);
+  for (uint32_t r = 0; r <= rows; ++r) {
+    t[(size_t)r * (cols + 1)] = 1;
+    for (uint32_t c = 1; c <= cols && c <= r; ++c)
+      t[(size_t)r * (cols + 1) + c] = t[(size_t)(r - 1) * (cols + 1) + c - 1] + t[(size_t)(r - 1) * (cols + 1) + c];
+  }
+  std::vector<unsigned long long> h(t.size() * 2);
+  for (size_t i = 0; i < t.size(); ++i) {
+    h[2 * i] = (unsigned long long)t[i];
+    h[2 * i + 1] = (unsigned long long)(t[i] >> 64);
+  }
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->d_binom) cudaFree(ctx->d_binom);
+  ctx->d_binom = nullptr;
+  KC_CUDA(cudaMalloc(&ctx->d_binom, h.size() * sizeof(unsigned long long)));
+  KC_CUDA(cudaMemcpy(ctx->d_binom, h.data(), h.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+  ctx->brows = rows;
+  ctx->bcols = cols;
+  return KC_OK;
+}
+
+void count_release(CountPlan* pl) {
+  cudaStream_t s = pl->g->ctx->stream;
+  for (int c = 0; c < kNumClasses; ++c) release_launch(pl->launches[c], s);
+  void* ps[] = {pl->size, pl->hist, pl->rev, pl->queue, pl->scratch};
+  for (void* p : ps)
+    if (p) cudaFreeAsync(p, s);
+  pl->size = pl->hist = pl->rev = pl->queue = pl->scratch = nullptr;
+}
+
+// Allocates the queue and the class launches. No kernel runs; the plan can be
+// enqueued (and captured) any number of times.
+kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long* d_out, uint32_t depth_boost,
+                        CountPlan* pl) {
+  kc_ctx* ctx = g->ctx;
+  cudaStream_t s = ctx->stream;
+  pl->g = g;
+  pl->req = req;
+  pl->edge = req.unit == KC_UNIT_EDGE;
+  pl->d_out = d_out;
+  const uint32_t k_max = std::max(req.k, req.k_max);
+  if (pl->edge) KC_TRY(ensure_edge_rows(g));
+  pl->n_units = pl->edge ? (uint32_t)g->m : g->n;
+  pl->max_size = g->max_out;
+  if (pl->max_size >= 65535u)
+    return fail(KC_ERR_INVALID_ARG, "largest out-degree %u exceeds the 65534 supported per unit", pl->max_size);
+  if (req.mode == KC_MODE_PIVOT) KC_TRY(ensure_binom(ctx, pl->max_size + 2, k_max + 1));
+  const uint32_t nu = std::max<uint32_t>(1, pl->n_units);
+  KC_CUDA(cudaMallocAsync(&pl->size, sizeof(uint32_t) * nu, s));
+  KC_CUDA(cudaMallocAsync(&pl->queue, sizeof(uint32_t) * nu, s));
+  KC_CUDA(cudaMallocAsync(&pl->hist, sizeof(uint32_t) * ((size_t)pl->max_size + 2), s));
+  KC_CUDA(cudaMallocAsync(&pl->rev, sizeof(uint32_t) * ((size_t)pl->max_size + 2), s));
+  KC_CUDA(cudaMallocAsync(&pl->scratch, sizeof(uint32_t) * 64, s));
+  for (int c = 0; c < kNumClasses; ++c) {
+    if ((int64_t)pl->max_size <= kClasses[c].lo) continue;
+    LaunchPlan lp;
+    lp.mode = req.mode;
+    lp.encoding = req.encoding;
+    lp.edge = pl->edge;
+    lp.dcap = (uint32_t)std::max<int64_t>(1, std::min<int64_t>(kClasses[c].hi, pl->max_size));
+    lp.G = kClasses[c].G;
+    lp.block = kClasses[c].block;
+    lp.force_global_bitmap = (c == 0);
+    lp.k_max = k_max;
+    lp.part = req.part ? req.part : auto_part(req.mode, (lp.dcap + 31) / 32);
+    lp.depth_boost = depth_boost;
+    CountParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.rp = g->drp;
+    p.col = g->dcol;
+    p.erow = g->erow;
+    p.queue = pl->queue;
+    p.bounds = pl->scratch + 32;
+    p.cls = (uint32_t)c;
+    p.n_units_max = pl->n_units;
+    p.edge_units = pl->edge ? 1 : 0;
+    p.vgraph = g->vgraph;
+    p.gk = req.d_graph_k;
+    p.k0 = req.k;
+    p.out = d_out;
+    p.binom = ctx->d_binom;
+    p.binom_cols = ctx->bcols;
+    p.ticket = pl->scratch + c;
+    p.err = pl->scratch + 8;
+    p.stats = (req.flags & KC_FLAG_STATS) ? reinterpret_cast<unsigned long long*>(pl->scratch + 16) : nullptr;
+    KC_TRY(prepare_launch(ctx, lp, p, s, &pl->launches[c]));
+    pl->active[c] = true;
+  }
+  return KC_OK;
+}
+
+// Enqueues queue construction and the class launches: no allocation, no
+// synchronisation, so the whole sequence can be captured in a CUDA graph.
+kc_status count_enqueue(const CountPlan& pl, cudaStream_t s) {
+  kc_graph* g = pl.g;
+  const int sms = g->ctx->sms;
+  const uint32_t M = pl.max_size;
+  KC_CUDA(cudaMemsetAsync(pl.hist, 0, sizeof(uint32_t) * ((size_t)M + 2), s));
+  KC_CUDA(cudaMemsetAsync(pl.scratch, 0, sizeof(uint32_t) * 32, s));
+  const uint32_t gq = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((pl.n_units + 255) / 256, (uint64_t)sms * 16));
+  if (pl.n_units)
+    k_unit_sizes<<<gq, 256, 0, s>>>(g->drp, g->dcol, g->erow, pl.n_units, pl.edge ? 1 : 0, g->vgraph,
+                                    pl.req.d_graph_k, pl.req.k, pl.size, pl.hist);
+  k_reverse<<<(M + 1 + 255) / 256, 256, 0, s>>>(pl.hist, M + 1, pl.rev);
+  KC_CUDA(prim::scan_exclusive_u32(pl.rev, pl.rev, M + 1, s));
+  k_class_bounds<<<1, 32, 0, s>>>(pl.rev, M, pl.scratch + 32);
+  if (pl.n_units) k_unit_scatter<<<gq, 256, 0, s>>>(pl.size, pl.n_units, M, pl.rev, pl.queue);
+  KC_CUDA(cudaGetLastError());
+  for (int c = 0; c < kNumClasses; ++c)
+    if (pl.active[c]) KC_TRY(enqueue_launch(pl.launches[c], s));
+  return KC_OK;
+}
+
+uint32_t count_error(const CountPlan& pl, cudaStream_t s, unsigned long long* stats3) {
+  uint32_t h[64];
+  cudaMemcpyAsync(h, pl.scratch, sizeof(h), cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  if (stats3) std::memcpy(stats3, h + 16, 3 * sizeof(unsigned long long));
+  return h[8];
+}
+
+uint64_t count_units(const CountPlan& pl, cudaStream_t s) {
+  uint32_t b[2 * kNumClasses];
+  cudaMemcpyAsync(b, pl.scratch + 32, sizeof(b), cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  uint64_t t = 0;
+  for (int c = 0; c < kNumClasses; ++c) t += b[2 * c + 1];
+  return t;
+}
+
+kc_status count_graph(kc_graph* g, const CountRequest& req, unsigned long long* d_out, kc_count_stats* stats) {
+  kc_ctx* ctx = g->ctx;
+  cudaStream_t s = ctx->stream;
+  cudaEvent_t ev0, ev1;
+  cudaEventCreate(&ev0);
+  cudaEventCreate(&ev1);
+  kc_status st = KC_OK;
+  uint32_t kernels = 0;
+  uint64_t units = 0;
+  unsigned long long sv[3] = {0, 0, 0};
+  for (uint32_t boost = 0; boost < 2; ++boost) {
+    CountPlan pl;
+    st = count_prepare(g, req, d_out, boost, &pl);
+    if (st == KC_OK) {
+      cudaEventRecord(ev0, s);
+      st = count_enqueue(pl, s);
+      cudaEventRecord(ev1, s);
+    }
+    uint32_t err = 0;
+    if (st == KC_OK) {
+      err = count_error(pl, s, sv);
+      units = count_units(pl, s);
+      kernels = 5;
+      for (int c = 0; c < kNumClasses; ++c) kernels += pl.active[c] ? 1 : 0;
+    }
+    count_release(&pl);
+    if (st != KC_OK) break;
+    if (err == DEV_ERR_STACK && boost == 0 && req.mode == KC_MODE_PIVOT) {
+      // a clique tree deeper than the fast stack: rerun with the full depth
+      KC_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long) * 2 * req.n_graphs, s));
+      continue;
+    }
+    if (err) st = fail(KC_ERR_INTERNAL, "counting kernel reported device error %u", err);
+    break;
+  }
+  if (stats && st == KC_OK) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    stats->units = units;
+    stats->tree_nodes = sv[0];
+    stats->word_ops = sv[1];
+    stats->gather_bytes = sv[2];
+    stats->ms_total = ms;
+    stats->ms_traversal = ms;
+    stats->max_unit_size = g->max_out;
+    stats->kernels = kernels;
+  }
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  return st;
+}
+
+}  // namespace kc

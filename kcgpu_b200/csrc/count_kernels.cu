@@ -1,0 +1,486 @@
+// Bitmap-encoded counting kernels (orientation and pivoting) and the launch
+// planner shared with the list-encoded kernels.
+//
+// One kernel body serves node and edge units; the unit only changes how the
+// vertex set S is formed:
+//   node unit u:     S = N+(u)                 (kckernels_orientation.cuh:357-377)
+//   edge unit u->v:  S = N+(u) ∩ N+(v)         (kckernels_orientation.cuh:518-555)
+// Orientation traversal (kckernels_orientation.cuh:380-470): every t-clique
+// (t = k-1 for node units, k-2 for edge units) of the DAG on S is counted
+// once from its lowest vertex; the last level is counted by popcount.
+// Pivot traversal (kckernels_pivoting.cuh:124-338): the succinct clique tree
+// with the max-neighbourhood pivot, ties to the smallest index; a leaf adds
+// C(drop, k - held) from an exact table (the reference parses doubles,
+// kclique/kclique.cuh:1694-1717).
+#include <algorithm>
+
+#include "count_kernels.cuh"
+#include "dev_common.cuh"
+
+namespace kc {
+
+namespace {
+
+struct Part {
+  uint32_t P, plane, pmask, pbase;
+};
+
+// First set bit of set[w0, W) (all lanes of the partition agree); -1 if none.
+__device__ __forceinline__ int part_next_bit(const uint32_t* set, uint32_t w0, uint32_t W, const Part& pt,
+                                             uint32_t* wi) {
+  for (uint32_t base = w0; base < W; base += pt.P) {
+    const uint32_t w = base + pt.plane;
+    const uint32_t x = w < W ? set[w] : 0u;
+    const uint32_t bal = (__ballot_sync(pt.pmask, x != 0u) & pt.pmask) >> pt.pbase;
+    if (bal) {
+      const uint32_t f = __ffs(bal) - 1;
+      const uint32_t xv = __shfl_sync(pt.pmask, x, pt.pbase + f);
+      *wi = base + f;
+      return (int)((base + f) * 32u + (uint32_t)__ffs(xv) - 1u);
+    }
+  }
+  return -1;
+}
+
+__device__ __forceinline__ uint32_t low_mask(uint32_t v, uint32_t w) {  // bits < v inside word w
+  const uint32_t vw = v >> 5;
+  return w < vw ? 0xffffffffu : (w == vw ? ((1u << (v & 31u)) - 1u) : 0u);
+}
+
+__device__ __forceinline__ uint32_t valid_mask(uint32_t d, uint32_t w) {  // bits < d inside word w
+  return low_mask(d, w);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  const uint32_t G = p.G;
+  const uint32_t gpb = blockDim.x / G;
+  const uint32_t gib = threadIdx.x / G;
+  const uint32_t gt = threadIdx.x - gib * G;
+  const uint32_t lane = lane_id();
+  const uint32_t wig = gt >> 5, nwg = G >> 5;
+  Part pt;
+  pt.P = p.P;
+  pt.plane = gt % p.P;
+  pt.pbase = (lane / p.P) * p.P;
+  pt.pmask = p.P >= 32 ? 0xffffffffu : (((1u << p.P) - 1u) << pt.pbase);
+  const uint32_t part = gt / p.P;
+
+  uint32_t* sb = smem + (size_t)gib * p.group_words;
+  uint32_t* gb = p.gbuf ? p.gbuf + (size_t)(blockIdx.x * gpb + gib) * p.gbuf_words : nullptr;
+  uint32_t* hdr = sb;
+  uint32_t* S = sb + 16;
+  uint32_t* B = p.bitmap_global ? gb : sb + p.off_B;
+  uint32_t* R0 = sb + p.off_R0;
+  uint32_t* frames = (p.frames_global ? gb + p.goff_fr : sb + p.off_fr) + (size_t)part * p.depth * p.fw;
+
+  // class bounds come from device memory: clamp them so no unit index can leave the queue
+  const uint32_t ubeg = min(p.bounds[2 * p.cls], p.n_units_max);
+  const uint32_t ucnt = min(p.bounds[2 * p.cls + 1], p.n_units_max - ubeg);
+  unsigned __int128 acc = 0;
+  uint32_t acc_graph = 0xffffffffu;
+  unsigned long long st_nodes = 0, st_words = 0, st_bytes = 0;
+
+  auto gsync = [&]() {
+    if (G == 32) __syncwarp(); else __syncthreads();
+  };
+  auto flush = [&]() {
+    if (pt.plane == 0 && acc != 0 && acc_graph != 0xffffffffu) atomic_add_u128(p.out + 2ull * acc_graph, acc);
+    acc = 0;
+  };
+
+  for (;;) {
+    if (gt == 0) {
+      hdr[0] = atomicAdd(p.ticket, 1u);
+      hdr[1] = 0;  // subtree ticket of this unit
+    }
+    gsync();
+    const uint32_t ui = hdr[0];
+    if (ui >= ucnt) break;
+    const uint32_t unit = p.queue[ubeg + ui];
+    uint32_t src, d;
+    if (!p.edge_units) {
+      src = unit;
+      const uint32_t b = p.rp[src];
+      d = p.rp[src + 1] - b;
+      if (d <= p.dcap)
+        for (uint32_t j = gt; j < d; j += G) S[j] = p.col[b + j];
+    } else {
+      src = p.erow[unit];
+      const uint32_t v = p.col[unit];
+      if (wig == 0) {
+        // S = N+(u) ∩ N+(v): stream the shorter list, search the longer
+        const uint32_t ub = p.rp[src], ue = p.rp[src + 1], vb = p.rp[v], ve = p.rp[v + 1];
+        const uint32_t *A, *L;
+        uint32_t la, ll;
+        if (ue - ub <= ve - vb) { A = p.col + ub; la = ue - ub; L = p.col + vb; ll = ve - vb; }
+        else { A = p.col + vb; la = ve - vb; L = p.col + ub; ll = ue - ub; }
+        uint32_t cnt = 0;
+        for (uint32_t i0 = 0; i0 < la; i0 += 32) {
+          const uint32_t i = i0 + lane;
+          bool found = false;
+          uint32_t x = 0;
+          if (i < la) {
+            x = A[i];
+            const uint32_t pos = lower_bound_u32(L, ll, x);
+            found = pos < ll && L[pos] == x;
+          }
+          const uint32_t bal = __ballot_sync(0xffffffffu, found);
+          if (found && cnt + __popc(bal & lanemask_lt()) < p.dcap) S[cnt + __popc(bal & lanemask_lt())] = x;
+          cnt += __popc(bal);
+        }
+        if (lane == 0) hdr[2] = cnt;
+        st_bytes += 4ull * (la + la * 8ull);
+      }
+      gsync();
+      d = hdr[2];
+    }
+    const uint32_t gph = p.vgraph ? p.vgraph[src] : 0u;
+    const uint32_t k = p.gk ? p.gk[gph] : p.k0;
+    gsync();
+    if (gph != acc_graph) {
+      flush();
+      acc_graph = gph;
+    }
+    if (d > p.dcap) {
+      if (gt == 0) set_error(p.err, DEV_ERR_CAPACITY);
+      gsync();
+      continue;
+    }
+    const uint32_t W = (d + 31u) >> 5;
+    const bool sym = MODE == 1;
+
+    if (MODE == 0) {
+      const uint32_t t = p.edge_units ? k - 2u : k - 1u;
+      if (t <= 1u || d < t) {
+        if (part == 0 && d >= t) acc += (t == 0u) ? 1u : d;
+        gsync();
+        continue;
+      }
+    } else {
+      const uint32_t hold0 = p.edge_units ? 2u : 1u;
+      if (d == 0u || hold0 + d < k) {
+        if (part == 0 && d == 0u && k == hold0) acc += 1u;
+        gsync();
+        continue;
+      }
+    }
+
+    // ---- induced subgraph on S as a bitmap (row j, bit i: S[i] in N+(S[j]))
+    for (uint32_t i = gt; i < d * W; i += G) B[i] = 0u;
+    gsync();
+    {
+      const uint32_t last = S[d - 1];
+      for (uint32_t j = wig; j < d; j += nwg) {
+        const uint32_t x0 = S[j];
+        const uint32_t b = p.rp[x0], e = p.rp[x0 + 1];
+        uint32_t i0 = b;
+        for (; i0 < e; i0 += 32) {
+          const uint32_t i = i0 + lane;
+          const uint32_t x = i < e ? __ldg(p.col + i) : 0xffffffffu;
+          const bool inr = x <= last;
+          if (!__any_sync(0xffffffffu, inr)) break;
+          if (inr) {
+            uint32_t lo = j + 1, hi = d;
+            while (lo < hi) {
+              const uint32_t mid = (lo + hi) >> 1;
+              if (S[mid] < x) lo = mid + 1; else hi = mid;
+            }
+            if (lo < d && S[lo] == x) {
+              atomicOr(&B[j * W + (lo >> 5)], 1u << (lo & 31u));
+              if (sym) atomicOr(&B[lo * W + (j >> 5)], 1u << (j & 31u));
+            }
+          }
+        }
+        st_bytes += 4ull * (min(i0 + 32u, e) - b);
+      }
+    }
+    gsync();
+
+    if (MODE == 0) {
+      // ---- orientation traversal
+      const uint32_t t = p.edge_units ? k - 2u : k - 1u;
+      for (;;) {
+        uint32_t j = 0;
+        if (pt.plane == 0) j = atomicAdd(&hdr[1], 1u);
+        j = __shfl_sync(pt.pmask, j, pt.pbase);
+        if (j >= d) break;
+        uint32_t* F0 = frames;
+        const uint32_t ws = j >> 5;
+        uint32_t c = 0;
+        for (uint32_t w = ws + pt.plane; w < W; w += pt.P) {
+          const uint32_t x = B[j * W + w];
+          F0[w] = x;
+          c += __popc(x);
+        }
+        c = __reduce_add_sync(pt.pmask, c);
+        st_nodes++;
+        st_words += W - ws;
+        if (t == 2u) { acc += c; continue; }
+        if (c < t - 1u) continue;
+        if (pt.plane == 0) F0[W] = ws;
+        __syncwarp(pt.pmask);
+        int lv = 0;
+        while (lv >= 0) {
+          uint32_t* F = frames + (size_t)lv * p.fw;
+          uint32_t wi = 0;
+          const int vb = part_next_bit(F, F[W], W, pt, &wi);
+          if (vb < 0) { --lv; continue; }
+          const uint32_t v = (uint32_t)vb;
+          __syncwarp(pt.pmask);
+          if (pt.plane == 0) { F[wi] &= ~(1u << (v & 31u)); F[W] = wi; }
+          __syncwarp(pt.pmask);
+          const uint32_t rem = t - (uint32_t)(lv + 2);
+          uint32_t* Fc = F + p.fw;
+          const bool store = rem > 1u && (uint32_t)(lv + 1) < p.depth;
+          uint32_t cc = 0;
+          for (uint32_t w = wi + pt.plane; w < W; w += pt.P) {
+            const uint32_t x = F[w] & B[v * W + w];
+            if (store) Fc[w] = x;
+            cc += __popc(x);
+          }
+          cc = __reduce_add_sync(pt.pmask, cc);
+          st_nodes++;
+          st_words += W - wi;
+          if (rem == 1u) {
+            acc += cc;
+          } else if (cc >= rem) {
+            if (!store) {
+              if (pt.plane == 0) set_error(p.err, DEV_ERR_STACK);
+            } else {
+              if (pt.plane == 0) Fc[W] = wi;
+              __syncwarp(pt.pmask);
+              ++lv;
+            }
+          }
+        }
+      }
+    } else {
+      // ---- pivot traversal (succinct clique tree)
+      const uint32_t hold0 = p.edge_units ? 2u : 1u;
+      uint32_t key = 0;
+      for (uint32_t v = gt; v < d; v += G) {
+        uint32_t c = 0;
+        for (uint32_t w = 0; w < W; ++w) c += __popc(B[v * W + w]);
+        key = max(key, (c << 16) | (0xffffu - v));
+      }
+      key = __reduce_max_sync(0xffffffffu, key);
+      if (lane == 0) hdr[8 + wig] = key;
+      gsync();
+      if (gt == 0) {
+        uint32_t m = 0;
+        for (uint32_t q = 0; q < nwg; ++q) m = max(m, hdr[8 + q]);
+        hdr[3] = 0xffffu - (m & 0xffffu);
+      }
+      gsync();
+      const uint32_t p0 = hdr[3];
+      for (uint32_t w = gt; w < W; w += G) R0[w] = ~B[p0 * W + w] & valid_mask(d, w);
+      gsync();
+
+      auto enter = [&](uint32_t* F, uint32_t hold, uint32_t drop) -> bool {
+        uint32_t nc = 0;
+        for (uint32_t w = pt.plane; w < W; w += pt.P) nc += __popc(F[w]);
+        nc = __reduce_add_sync(pt.pmask, nc);
+        if (nc == 0u) {
+          if (hold <= k && hold + drop >= k) {
+            const unsigned long long* e = p.binom + 2ull * ((size_t)drop * (p.binom_cols + 1u) + (k - hold));
+            acc += ((unsigned __int128)e[1] << 64) | e[0];
+          }
+          return false;
+        }
+        if (hold + drop + nc < k) return false;
+        uint32_t best = 0;
+        if (W <= 4u) {
+          uint32_t idx = 0;
+          for (uint32_t w = 0; w < W; ++w) {
+            uint32_t x = F[w];
+            while (x) {
+              const uint32_t b = __ffs(x) - 1u;
+              x &= x - 1u;
+              if ((idx++ % pt.P) == pt.plane) {
+                const uint32_t u = w * 32u + b;
+                uint32_t c = 0;
+                for (uint32_t q = 0; q < W; ++q) c += __popc(F[q] & B[u * W + q]);
+                best = max(best, (c << 16) | (0xffffu - u));
+              }
+            }
+          }
+          st_words += (unsigned long long)nc * W / pt.P;
+        } else {
+          for (uint32_t w = 0; w < W; ++w) {
+            uint32_t x = F[w];
+            while (x) {
+              const uint32_t b = __ffs(x) - 1u;
+              x &= x - 1u;
+              const uint32_t u = w * 32u + b;
+              uint32_t c = 0;
+              for (uint32_t q = pt.plane; q < W; q += pt.P) c += __popc(F[q] & B[u * W + q]);
+              c = __reduce_add_sync(pt.pmask, c);
+              best = max(best, (c << 16) | (0xffffu - u));
+            }
+          }
+          st_words += (unsigned long long)nc * W;
+        }
+        best = __reduce_max_sync(pt.pmask, best);
+        const uint32_t piv = 0xffffu - (best & 0xffffu);
+        for (uint32_t w = pt.plane; w < W; w += pt.P) F[W + w] = F[w] & ~B[piv * W + w];
+        __syncwarp(pt.pmask);
+        if (pt.plane == 0) {
+          F[2 * W] = hold;
+          F[2 * W + 1] = drop;
+          F[2 * W + 2] = piv;
+          F[2 * W + 3] = 0;
+        }
+        __syncwarp(pt.pmask);
+        return true;
+      };
+
+      for (;;) {
+        uint32_t v = 0;
+        if (pt.plane == 0) v = atomicAdd(&hdr[1], 1u);
+        v = __shfl_sync(pt.pmask, v, pt.pbase);
+        if (v >= d) break;
+        if (!((R0[v >> 5] >> (v & 31u)) & 1u)) continue;
+        const uint32_t hold = hold0 + (v != p0 ? 1u : 0u), drop = (v == p0) ? 1u : 0u;
+        st_nodes++;
+        if (hold > k) continue;
+        uint32_t* F0 = frames;
+        for (uint32_t w = pt.plane; w < W; w += pt.P) F0[w] = B[v * W + w] & ~(R0[w] & low_mask(v, w));
+        __syncwarp(pt.pmask);
+        if (!enter(F0, hold, drop)) continue;
+        int lv = 0;
+        while (lv >= 0) {
+          uint32_t* F = frames + (size_t)lv * p.fw;
+          uint32_t wi = 0;
+          const int vb = part_next_bit(F + W, F[2 * W + 3], W, pt, &wi);
+          if (vb < 0) { --lv; continue; }
+          const uint32_t u = (uint32_t)vb;
+          const uint32_t fh = F[2 * W], fd = F[2 * W + 1], fp = F[2 * W + 2];
+          __syncwarp(pt.pmask);
+          if (pt.plane == 0) {
+            F[W + wi] &= ~(1u << (u & 31u));
+            F[2 * W + 3] = wi;
+          }
+          const uint32_t h2 = fh + (u != fp ? 1u : 0u), d2 = fd + (u == fp ? 1u : 0u);
+          st_nodes++;
+          bool descend = h2 <= k;
+          if (descend && (uint32_t)(lv + 1) >= p.depth) {
+            if (pt.plane == 0) set_error(p.err, DEV_ERR_STACK);
+            descend = false;
+          }
+          uint32_t* Fc = F + p.fw;
+          if (descend)
+            for (uint32_t w = pt.plane; w < W; w += pt.P) Fc[w] = F[w] & B[u * W + w];
+          __syncwarp(pt.pmask);
+          if (pt.plane == 0) F[u >> 5] &= ~(1u << (u & 31u));  // later siblings exclude u
+          __syncwarp(pt.pmask);
+          if (descend && enter(Fc, h2, d2)) ++lv;
+        }
+      }
+    }
+    gsync();
+  }
+  flush();
+  if (p.stats && pt.plane == 0) {
+    atomicAdd(p.stats + 0, st_nodes);
+    atomicAdd(p.stats + 1, st_words);
+    if (part == 0) atomicAdd(p.stats + 2, st_bytes);
+  }
+}
+
+}  // namespace
+
+kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p0, cudaStream_t s,
+                         PreparedLaunch* out) {
+  if (lp.encoding == KC_ENC_LIST) return prepare_launch_list(ctx, lp, p0, s, out);
+  CountParams p = p0;
+  const uint32_t P = lp.part;
+  if (P == 0 || P > 32 || (P & (P - 1)) != 0)
+    return fail(KC_ERR_INVALID_ARG, "partition size %u is not one of 1,2,4,8,16,32", P);
+  const uint32_t G = lp.G, block = lp.block;
+  const uint32_t dcap = std::max<uint32_t>(1, lp.dcap);
+  const uint32_t W = (dcap + 31) / 32;
+  const uint32_t nparts = G / P;
+  const uint32_t gpb = block / G;
+  uint32_t depth, fw;
+  if (lp.mode == KC_MODE_ORIENT) {
+    const uint32_t t = lp.edge ? (lp.k_max >= 2 ? lp.k_max - 2 : 0) : lp.k_max - 1;
+    depth = std::max<uint32_t>(1, t >= 2 ? t - 2 : 1);
+    fw = W + 1;
+  } else {
+    depth = lp.depth_boost ? dcap + 2 : std::min<uint32_t>(dcap + 2, 64);
+    fw = 2 * W + 4;
+  }
+  auto al4 = [](size_t x) { return (x + 3) & ~(size_t)3; };
+  const size_t hdr = 16, sS = al4(dcap), sR0 = al4(W);
+  const size_t sB = (size_t)dcap * W;
+  const size_t sFr = (size_t)nparts * depth * fw;
+  const size_t limit_words = (size_t)ctx->max_smem_optin / 4;
+  bool bitmap_global = lp.force_global_bitmap;
+  bool frames_global = false;
+  auto group_words = [&]() {
+    return hdr + sS + sR0 + (bitmap_global ? 0 : al4(sB)) + (frames_global ? 0 : sFr);
+  };
+  if ((size_t)gpb * group_words() > limit_words) frames_global = true;
+  if ((size_t)gpb * group_words() > limit_words) bitmap_global = true;
+  if ((size_t)gpb * group_words() > limit_words)
+    return fail(KC_ERR_INVALID_ARG, "unit size %u does not fit the shared-memory plan", dcap);
+  p.dcap = dcap;
+  p.W = W;
+  p.P = P;
+  p.G = G;
+  p.depth = depth;
+  p.fw = fw;
+  p.group_words = (uint32_t)group_words();
+  p.off_B = (uint32_t)(hdr + sS + sR0);
+  p.off_R0 = (uint32_t)(hdr + sS);
+  p.off_fr = (uint32_t)(hdr + sS + sR0 + (bitmap_global ? 0 : al4(sB)));
+  p.bitmap_global = bitmap_global;
+  p.frames_global = frames_global;
+  p.gbuf_words = (bitmap_global ? al4(sB) : 0) + (frames_global ? sFr : 0);
+  p.goff_fr = bitmap_global ? al4(sB) : 0;
+  p.gbuf = nullptr;
+
+  const size_t smem_bytes = (size_t)gpb * p.group_words * 4;
+  auto kern = lp.mode == KC_MODE_ORIENT ? k_count_bitmap<0> : k_count_bitmap<1>;
+  // Several classes launch the same kernel with different shared-memory sizes;
+  // the attribute is per function, so it is set to the device maximum.
+  KC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->max_smem_optin));
+  int per_sm = 0;
+  KC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, smem_bytes));
+  per_sm = std::max(1, per_sm);
+  uint64_t grid = std::min<uint64_t>((uint64_t)ctx->sms * per_sm, ((uint64_t)p.n_units_max + gpb - 1) / gpb);
+  grid = std::max<uint64_t>(1, grid);
+  if (p.gbuf_words) {
+    // keep the global scratch of the whole grid within 24 GiB
+    const uint64_t per_block = (uint64_t)gpb * p.gbuf_words * 4;
+    const uint64_t cap = std::max<uint64_t>(1, (24ull << 30) / std::max<uint64_t>(1, per_block));
+    grid = std::min(grid, cap);
+    KC_CUDA(cudaMallocAsync(&out->gbuf, grid * per_block, s));
+    p.gbuf = out->gbuf;
+  }
+  out->p = p;
+  out->grid = (uint32_t)grid;
+  out->block = block;
+  out->smem = smem_bytes;
+  out->kernel = (void*)kern;
+  out->list = false;
+  return KC_OK;
+}
+
+kc_status enqueue_launch(const PreparedLaunch& pl, cudaStream_t s) {
+  CountParams p = pl.p;
+  size_t cap = pl.cap_edges;
+  void* args_bitmap[] = {&p};
+  void* args_list[] = {&p, &cap};
+  KC_CUDA(cudaLaunchKernel(pl.kernel, dim3(pl.grid), dim3(pl.block), pl.list ? args_list : args_bitmap, pl.smem, s));
+  return KC_OK;
+}
+
+void release_launch(PreparedLaunch& pl, cudaStream_t s) {
+  if (pl.gbuf) cudaFreeAsync(pl.gbuf, s);
+  pl.gbuf = nullptr;
+}
+
+}  // namespace kc

@@ -1,0 +1,98 @@
+// Launch plan and kernel parameters of the counting kernels.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "engine.h"
+
+namespace kc {
+
+// Everything a counting kernel reads; plain pointers, filled on the host.
+struct CountParams {
+  const uint32_t* rp;        // DAG row pointer (rank labels)
+  const uint32_t* col;       // DAG columns, sorted per row
+  const uint32_t* erow;      // source of every DAG edge (edge units)
+  const uint32_t* queue;     // all units, largest first
+  const uint32_t* bounds;    // device [begin, count] per size class
+  uint32_t cls;              // this launch's class
+  uint32_t n_units_max;      // host upper bound on the class size (grid sizing)
+  uint32_t edge_units;       // 0 node units, 1 edge units
+  const uint32_t* vgraph;    // graph of every rank label, or null
+  const uint32_t* gk;        // k of every graph, or null
+  uint32_t k0;               // k when gk is null
+  unsigned long long* out;   // (lo, hi) per graph
+  const unsigned long long* binom;  // C(r, c) as (lo, hi), row stride binom_cols + 1
+  uint32_t binom_cols;
+  uint32_t dcap;             // largest |S| of this launch
+  uint32_t W;                // words per bitmap row at dcap
+  uint32_t P;                // lanes per partition
+  uint32_t G;                // threads per unit group (32 or blockDim.x)
+  uint32_t depth;            // traversal stack frames per partition
+  uint32_t fw;               // words per frame
+  uint32_t group_words;      // shared-memory words per group
+  uint32_t off_B, off_R0, off_fr;  // shared-memory offsets (words) inside a group
+  uint32_t bitmap_global, frames_global;
+  uint32_t* gbuf;            // global scratch, gbuf_words per group
+  size_t gbuf_words;
+  size_t goff_fr;            // frames offset inside a group's global scratch
+  uint32_t* ticket;          // unit ticket (zeroed)
+  uint32_t* err;             // device error word
+  unsigned long long* stats; // [0] tree nodes [1] word-ops [2] gather bytes, or null
+};
+
+struct LaunchPlan {
+  uint32_t mode = 0, encoding = 0, part = 0;
+  bool edge = false;
+  uint32_t dcap = 0, G = 32, block = 128;
+  bool force_global_bitmap = false;
+  uint32_t k_max = 0;
+  uint32_t depth_boost = 0;
+};
+
+// A prepared launch: parameters, grid and the scratch it owns.
+struct PreparedLaunch {
+  CountParams p;
+  uint32_t grid = 0, block = 0;
+  size_t smem = 0;
+  void* kernel = nullptr;     // __global__ function
+  uint32_t* gbuf = nullptr;   // global scratch (freed by release_launch)
+  bool list = false;
+  size_t cap_edges = 0;       // list encoding: edge capacity per group
+};
+
+// Lays out shared/global scratch for the plan, sizes the persistent grid and
+// allocates the global scratch (stream-ordered on s). No kernel is launched.
+kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p, cudaStream_t s,
+                         PreparedLaunch* out);
+kc_status prepare_launch_list(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p, cudaStream_t s,
+                              PreparedLaunch* out);
+// Enqueues the kernel (capturable: no allocation, no synchronisation).
+kc_status enqueue_launch(const PreparedLaunch& pl, cudaStream_t s);
+void release_launch(PreparedLaunch& pl, cudaStream_t s);
+
+// Unit-size classes of the persistent queue.
+constexpr int kNumClasses = 4;
+
+// Everything one counting pass needs, allocated once; enqueue may be
+// repeated and captured in a CUDA graph.
+struct CountPlan {
+  kc_graph* g = nullptr;
+  CountRequest req;
+  bool edge = false;
+  uint32_t n_units = 0, max_size = 0;
+  uint32_t *size = nullptr, *hist = nullptr, *rev = nullptr, *queue = nullptr, *scratch = nullptr;
+  unsigned long long* d_out = nullptr;
+  PreparedLaunch launches[kNumClasses];
+  bool active[kNumClasses] = {false, false, false, false};
+};
+
+kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long* d_out, uint32_t depth_boost,
+                        CountPlan* pl);
+kc_status count_enqueue(const CountPlan& pl, cudaStream_t s);
+void count_release(CountPlan* pl);
+// Reads the device error word (and the three stats counters when stats3 != null).
+uint32_t count_error(const CountPlan& pl, cudaStream_t s, unsigned long long* stats3);
+uint64_t count_units(const CountPlan& pl, cudaStream_t s);
+
+}  // namespace kc

@@ -1,0 +1,466 @@
+// The C ABI of the engine (include/kc.h): contexts, graphs, orientation,
+// counting, k-core and k-truss support. Batched counting is in batch.cu and
+// the request server in server.cpp.
+//
+// Every entry point returns a kc_status, records a message for kc_last_error()
+// and never exits the process (the reference prints and continues on CUDA
+// errors, include/utils.cuh:44-51, and exits on bad flags, include/Config.h:88-89).
+#include <algorithm>
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "dev_common.cuh"
+#include "engine.h"
+#include "prims.cuh"
+
+namespace kc {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+kc_status fail(kc_status st, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return st;
+}
+
+void clear_error() { g_last_error.clear(); }
+
+kc_status cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
+  cudaGetLastError();
+  const char* base = std::strrchr(file, '/');
+  base = base ? base + 1 : file;
+  kc_status st = (e == cudaErrorMemoryAllocation) ? KC_ERR_OOM : KC_ERR_CUDA;
+  return fail(st, "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), base, line);
+}
+
+kc_status dev_alloc(kc_graph* g, void** p, size_t bytes) {
+  bytes = std::max<size_t>(bytes, 4);
+  cudaError_t e = cudaMallocAsync(p, bytes, g->ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "device allocation", __FILE__, __LINE__);
+  g->bytes += bytes;
+  return KC_OK;
+}
+
+void dev_free(kc_graph* g, void* p) {
+  if (p) cudaFreeAsync(p, g->ctx->stream);
+}
+
+namespace {
+
+__global__ void k_expand_rows(const uint32_t* __restrict__ rp, uint32_t n, uint32_t* src) {
+  const uint32_t lane = lane_id();
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t u = gw; u < n; u += nw)
+    for (uint32_t i = rp[u] + lane; i < rp[u + 1]; i += 32) src[i] = u;
+}
+
+struct CtxLock {
+  kc_ctx* c;
+  explicit CtxLock(kc_ctx* ctx) : c(ctx) {
+    c->mu.lock();
+    cudaSetDevice(c->device);
+    clear_error();
+  }
+  ~CtxLock() { c->mu.unlock(); }
+};
+
+void free_graph_arrays(kc_graph* g) {
+  void* ps[] = {g->rp, g->col, g->rank, g->inv, g->drp, g->dcol, g->erow, g->prio, g->level, g->vgraph};
+  for (void* p : ps)
+    if (p) cudaFreeAsync(p, g->ctx->stream);
+  g->rp = g->col = g->rank = g->inv = g->drp = g->dcol = g->erow = g->prio = g->level = g->vgraph = nullptr;
+}
+
+kc_status new_graph(kc_ctx* ctx, kc_graph** out) {
+  if (!out) return fail(KC_ERR_INVALID_ARG, "output pointer is NULL");
+  *out = nullptr;
+  kc_graph* g = new (std::nothrow) kc_graph();
+  if (!g) return fail(KC_ERR_OOM, "host allocation failed");
+  g->ctx = ctx;
+  *out = g;
+  return KC_OK;
+}
+
+kc_status build_from_device(kc_graph* g, const uint32_t* d_src, const uint32_t* d_dst, uint64_t E, uint32_t n) {
+  kc_status st = build_csr(g, d_src, d_dst, E, n);
+  if (st != KC_OK) return st;
+  return KC_OK;
+}
+
+}  // namespace
+
+kc_params autotune(uint32_t n, uint64_t m, uint32_t max_out, uint32_t k, uint32_t max_core) {
+  // Per-graph choice from shape features. Pivoting wins when the graph holds
+  // large cliques (its cost follows the clique tree, not the clique count);
+  // orientation listing wins on sparse graphs with few cliques. Word-width of
+  // the largest unit picks the partition size; edge units spread the work of
+  // graphs with few vertices but wide out-neighbourhoods.
+  kc_params p;
+  std::memset(&p, 0, sizeof(p));
+  p.k = k;
+  const double dens = n > 1 ? (2.0 * (double)m) / ((double)n * (n - 1)) : 0.0;
+  const bool dense_core = max_core >= 16 || (max_core + 1 >= k && k >= 7);
+  p.mode = (dense_core || k >= 9) ? KC_MODE_PIVOT : KC_MODE_ORIENT;
+  p.unit = (n < 256 && max_out > 64) ? KC_UNIT_EDGE : KC_UNIT_NODE;
+  const uint32_t W = (max_out + 31) / 32;
+  if (p.mode == KC_MODE_ORIENT) p.part = W <= 1 ? 1 : (W <= 2 ? 2 : (W <= 4 ? 4 : (W <= 8 ? 8 : 16)));
+  else p.part = W <= 2 ? 4 : (W <= 4 ? 8 : (W <= 8 ? 16 : 32));
+  p.encoding = (max_out > 4096 && dens < 0.001) ? KC_ENC_LIST : KC_ENC_BITMAP;
+  return p;
+}
+
+kc_status export_dag(kc_graph* g, uint32_t* h_rp, uint32_t* h_col);  // orient.cu
+
+}  // namespace kc
+
+using kc::fail;
+
+namespace {
+std::atomic<uint64_t> g_launches{0};
+}
+
+extern "C" {
+
+// Every kernel launch of this library goes through cudaLaunchKernel (the
+// <<<>>> stubs) or cudaLaunchCooperativeKernel; the link step wraps both
+// (-Wl,--wrap) so the launches can be counted.
+cudaError_t __real_cudaLaunchKernel(const void* f, dim3 g, dim3 b, void** a, size_t sm, cudaStream_t s);
+cudaError_t __wrap_cudaLaunchKernel(const void* f, dim3 g, dim3 b, void** a, size_t sm, cudaStream_t s) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return __real_cudaLaunchKernel(f, g, b, a, sm, s);
+}
+cudaError_t __real_cudaLaunchCooperativeKernel(const void* f, dim3 g, dim3 b, void** a, size_t sm, cudaStream_t s);
+cudaError_t __wrap_cudaLaunchCooperativeKernel(const void* f, dim3 g, dim3 b, void** a, size_t sm,
+                                               cudaStream_t s) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return __real_cudaLaunchCooperativeKernel(f, g, b, a, sm, s);
+}
+
+uint64_t kc_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
+
+const char* kc_last_error(void) { return kc::g_last_error.c_str(); }
+
+const char* kc_status_string(kc_status s) {
+  switch (s) {
+    case KC_OK: return "ok";
+    case KC_ERR_INVALID_ARG: return "invalid argument";
+    case KC_ERR_OOM: return "out of memory";
+    case KC_ERR_ADMISSION: return "admission rejected";
+    case KC_ERR_DEVICE_TIMEOUT: return "device wait timed out";
+    case KC_ERR_CUDA: return "CUDA error";
+    case KC_ERR_INTERNAL: return "internal error";
+    case KC_ERR_NOT_ORIENTED: return "graph not oriented";
+    case KC_ERR_CANCELLED: return "cancelled";
+    case KC_ERR_BUSY: return "busy";
+  }
+  return "unknown status";
+}
+
+kc_status kc_ctx_create(int device, kc_ctx** out) {
+  kc::clear_error();
+  if (!out) return fail(KC_ERR_INVALID_ARG, "output pointer is NULL");
+  *out = nullptr;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(KC_ERR_CUDA, "no CUDA device available (%s)", cudaGetErrorString(e));
+  }
+  if (device < 0 || device >= ndev) return fail(KC_ERR_INVALID_ARG, "device %d out of range [0,%d)", device, ndev);
+  kc_ctx* c = new (std::nothrow) kc_ctx();
+  if (!c) return fail(KC_ERR_OOM, "host allocation failed");
+  c->device = device;
+  KC_CUDA(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  KC_CUDA(cudaGetDeviceProperties(&prop, device));
+  c->sms = prop.multiProcessorCount;
+  c->max_smem_optin = (int)prop.sharedMemPerBlockOptin;
+  c->total_mem = prop.totalGlobalMem;
+  KC_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  // keep freed stream-ordered memory in the pool between calls
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  *out = c;
+  return KC_OK;
+}
+
+kc_status kc_ctx_destroy(kc_ctx* ctx) {
+  if (!ctx) return KC_OK;
+  {
+    std::lock_guard<std::mutex> l(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->d_binom) cudaFree(ctx->d_binom);
+    cudaStreamDestroy(ctx->stream);
+  }
+  delete ctx;
+  return KC_OK;
+}
+
+kc_status kc_ctx_set_spin_budget(kc_ctx* ctx, uint64_t ticks) {
+  if (!ctx) return fail(KC_ERR_INVALID_ARG, "context is NULL");
+  ctx->spin_budget = ticks;
+  return KC_OK;
+}
+
+kc_status kc_ctx_get_stream(kc_ctx* ctx, void** stream) {
+  if (!ctx || !stream) return fail(KC_ERR_INVALID_ARG, "NULL argument");
+  *stream = (void*)ctx->stream;
+  return KC_OK;
+}
+
+kc_status kc_graph_from_edges(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, uint64_t n_edges,
+                              uint32_t n_nodes, kc_graph** out) {
+  if (!ctx) return fail(KC_ERR_INVALID_ARG, "context is NULL");
+  if (n_edges && (!src || !dst)) return fail(KC_ERR_INVALID_ARG, "edge arrays are NULL");
+  kc::CtxLock lock(ctx);
+  kc_graph* g;
+  KC_TRY(kc::new_graph(ctx, &g));
+  cudaStream_t s = ctx->stream;
+  uint32_t *ds = nullptr, *dd = nullptr;
+  size_t bytes = std::max<uint64_t>(1, n_edges) * sizeof(uint32_t);
+  cudaError_t e1 = cudaMallocAsync(&ds, bytes, s), e2 = cudaMallocAsync(&dd, bytes, s);
+  if (e1 != cudaSuccess || e2 != cudaSuccess) {
+    delete g;
+    return kc::cuda_fail(e1 != cudaSuccess ? e1 : e2, "edge staging allocation", __FILE__, __LINE__);
+  }
+  if (n_edges) {
+    cudaMemcpyAsync(ds, src, n_edges * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dd, dst, n_edges * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+  }
+  kc_status st = kc::build_from_device(g, ds, dd, n_edges, n_nodes);
+  cudaFreeAsync(ds, s);
+  cudaFreeAsync(dd, s);
+  if (st != KC_OK) {
+    kc::free_graph_arrays(g);
+    delete g;
+    return st;
+  }
+  *out = g;
+  return KC_OK;
+}
+
+kc_status kc_graph_from_edges_device(kc_ctx* ctx, const uint32_t* d_src, const uint32_t* d_dst, uint64_t n_edges,
+                                     uint32_t n_nodes, kc_graph** out) {
+  if (!ctx) return fail(KC_ERR_INVALID_ARG, "context is NULL");
+  if (n_edges && (!d_src || !d_dst)) return fail(KC_ERR_INVALID_ARG, "edge arrays are NULL");
+  kc::CtxLock lock(ctx);
+  kc_graph* g;
+  KC_TRY(kc::new_graph(ctx, &g));
+  kc_status st = kc::build_from_device(g, d_src, d_dst, n_edges, n_nodes);
+  if (st != KC_OK) {
+    kc::free_graph_arrays(g);
+    delete g;
+    return st;
+  }
+  *out = g;
+  return KC_OK;
+}
+
+kc_status kc_graph_from_csr(kc_ctx* ctx, const uint32_t* row_ptr, const uint32_t* col_ind, uint32_t n_nodes,
+                            kc_graph** out) {
+  if (!ctx) return fail(KC_ERR_INVALID_ARG, "context is NULL");
+  if (!row_ptr) return fail(KC_ERR_INVALID_ARG, "row_ptr is NULL");
+  const uint64_t nnz = row_ptr[n_nodes];
+  if (nnz && !col_ind) return fail(KC_ERR_INVALID_ARG, "col_ind is NULL");
+  for (uint32_t v = 0; v < n_nodes; ++v)
+    if (row_ptr[v + 1] < row_ptr[v]) return fail(KC_ERR_INVALID_ARG, "row_ptr decreases at row %u", v);
+  kc::CtxLock lock(ctx);
+  kc_graph* g;
+  KC_TRY(kc::new_graph(ctx, &g));
+  cudaStream_t s = ctx->stream;
+  uint32_t *drp = nullptr, *ds = nullptr, *dd = nullptr;
+  KC_CUDA(cudaMallocAsync(&drp, sizeof(uint32_t) * ((size_t)n_nodes + 1), s));
+  KC_CUDA(cudaMallocAsync(&ds, sizeof(uint32_t) * std::max<uint64_t>(1, nnz), s));
+  KC_CUDA(cudaMallocAsync(&dd, sizeof(uint32_t) * std::max<uint64_t>(1, nnz), s));
+  KC_CUDA(cudaMemcpyAsync(drp, row_ptr, sizeof(uint32_t) * ((size_t)n_nodes + 1), cudaMemcpyHostToDevice, s));
+  if (nnz) KC_CUDA(cudaMemcpyAsync(dd, col_ind, sizeof(uint32_t) * nnz, cudaMemcpyHostToDevice, s));
+  if (n_nodes)
+    kc::k_expand_rows<<<std::max(1u, std::min((n_nodes * 32u + 255u) / 256u, (uint32_t)ctx->sms * 32)), 256, 0, s>>>(
+        drp, n_nodes, ds);
+  kc_status st = kc::build_from_device(g, ds, dd, nnz, n_nodes);
+  cudaFreeAsync(drp, s);
+  cudaFreeAsync(ds, s);
+  cudaFreeAsync(dd, s);
+  if (st != KC_OK) {
+    kc::free_graph_arrays(g);
+    delete g;
+    return st;
+  }
+  *out = g;
+  return KC_OK;
+}
+
+kc_status kc_graph_destroy(kc_graph* g) {
+  if (!g) return KC_OK;
+  kc::CtxLock lock(g->ctx);
+  kc::free_graph_arrays(g);
+  cudaStreamSynchronize(g->ctx->stream);
+  delete g;
+  return KC_OK;
+}
+
+kc_status kc_graph_get_info(const kc_graph* g, kc_graph_info* out) {
+  if (!g || !out) return fail(KC_ERR_INVALID_ARG, "NULL argument");
+  out->n = g->n;
+  out->m = g->m;
+  out->max_degree = g->max_deg;
+  out->oriented = g->oriented < 0 ? 0u : (uint32_t)g->oriented + 1u;
+  out->max_out_degree = g->max_out;
+  out->max_core = g->max_core;
+  out->device_bytes = g->bytes;
+  return KC_OK;
+}
+
+kc_status kc_graph_get_csr(const kc_graph* g, uint32_t* row_ptr, uint32_t* col_ind) {
+  if (!g || !row_ptr || (g->m && !col_ind)) return fail(KC_ERR_INVALID_ARG, "NULL argument");
+  kc::CtxLock lock(g->ctx);
+  cudaStream_t s = g->ctx->stream;
+  KC_CUDA(cudaMemcpyAsync(row_ptr, g->rp, sizeof(uint32_t) * ((size_t)g->n + 1), cudaMemcpyDeviceToHost, s));
+  if (g->m) KC_CUDA(cudaMemcpyAsync(col_ind, g->col, sizeof(uint32_t) * 2 * g->m, cudaMemcpyDeviceToHost, s));
+  KC_CUDA(cudaStreamSynchronize(s));
+  return KC_OK;
+}
+
+kc_status kc_orient(kc_graph* g, uint32_t orientation) {
+  if (!g) return fail(KC_ERR_INVALID_ARG, "graph is NULL");
+  kc::CtxLock lock(g->ctx);
+  return kc::orient_graph(g, orientation);
+}
+
+kc_status kc_graph_get_dag(const kc_graph* g, uint32_t* row_ptr, uint32_t* col_ind) {
+  if (!g || !row_ptr || (g->m && !col_ind)) return fail(KC_ERR_INVALID_ARG, "NULL argument");
+  if (g->oriented < 0) return fail(KC_ERR_NOT_ORIENTED, "call kc_orient first");
+  kc::CtxLock lock(g->ctx);
+  return kc::export_dag(const_cast<kc_graph*>(g), row_ptr, col_ind);
+}
+
+kc_status kc_graph_get_peel(const kc_graph* g, uint32_t* priority, uint32_t* level) {
+  if (!g) return fail(KC_ERR_INVALID_ARG, "graph is NULL");
+  if (!g->prio) return fail(KC_ERR_NOT_ORIENTED, "no degeneracy peel has run on this graph");
+  kc::CtxLock lock(g->ctx);
+  cudaStream_t s = g->ctx->stream;
+  if (priority && g->n) KC_CUDA(cudaMemcpyAsync(priority, g->prio, sizeof(uint32_t) * g->n, cudaMemcpyDeviceToHost, s));
+  if (level && g->n) KC_CUDA(cudaMemcpyAsync(level, g->level, sizeof(uint32_t) * g->n, cudaMemcpyDeviceToHost, s));
+  KC_CUDA(cudaStreamSynchronize(s));
+  return KC_OK;
+}
+
+kc_status kc_parse_spec(const char* spec, kc_params* io) {
+  // include/Config.h:235-271: [o|p]<digits>[b|n|h]; strings of length <= 2
+  // keep the defaults (orientation, partition 8, bitmap).
+  if (!io) return fail(KC_ERR_INVALID_ARG, "params pointer is NULL");
+  io->mode = KC_MODE_ORIENT;
+  io->part = 8;
+  io->encoding = KC_ENC_BITMAP;
+  if (!spec) return KC_OK;
+  const size_t len = std::strlen(spec);
+  if (len <= 2) return KC_OK;
+  if (spec[0] == 'p') io->mode = KC_MODE_PIVOT;
+  size_t i = 1;
+  uint32_t part = 0;
+  if (spec[i] < '0' || spec[i] > '9') return fail(KC_ERR_INVALID_ARG, "spec '%s': partition size expected", spec);
+  while (i < len && spec[i] >= '0' && spec[i] <= '9') part = part * 10 + (uint32_t)(spec[i++] - '0');
+  if (part == 0 || part > 32 || (part & (part - 1)))
+    return fail(KC_ERR_INVALID_ARG, "spec '%s': partition size %u is not one of 1,2,4,8,16,32", spec, part);
+  io->part = part;
+  if (i < len && spec[i] == 'n') io->encoding = KC_ENC_LIST;
+  return KC_OK;
+}
+
+kc_status kc_count(kc_graph* g, const kc_params* p, kc_u128* out, kc_count_stats* stats) {
+  if (!g || !p || !out) return fail(KC_ERR_INVALID_ARG, "NULL argument");
+  if (p->k < 1) return fail(KC_ERR_INVALID_ARG, "k must be >= 1");
+  if (p->mode > KC_MODE_PIVOT || p->unit > KC_UNIT_EDGE || p->encoding > KC_ENC_LIST)
+    return fail(KC_ERR_INVALID_ARG, "unknown mode, unit or encoding");
+  if (p->part != 0 && (p->part > 32 || (p->part & (p->part - 1))))
+    return fail(KC_ERR_INVALID_ARG, "partition size %u is not one of 1,2,4,8,16,32", p->part);
+  if (g->oriented < 0) return fail(KC_ERR_NOT_ORIENTED, "call kc_orient before kc_count");
+  kc::CtxLock lock(g->ctx);
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  out->lo = out->hi = 0;
+  if (p->k == 1) { out->lo = g->n; return KC_OK; }
+  if (p->k == 2) { out->lo = g->m; return KC_OK; }
+  cudaStream_t s = g->ctx->stream;
+  unsigned long long* d_out = nullptr;
+  KC_CUDA(cudaMallocAsync(&d_out, 2 * sizeof(unsigned long long), s));
+  KC_CUDA(cudaMemsetAsync(d_out, 0, 2 * sizeof(unsigned long long), s));
+  kc::CountRequest req;
+  req.k = p->k;
+  req.mode = p->mode;
+  req.unit = p->unit;
+  req.part = p->part;
+  req.encoding = p->encoding;
+  req.flags = p->flags;
+  req.k_max = p->k;
+  kc_status st = kc::count_graph(g, req, d_out, (p->flags & KC_FLAG_STATS) ? stats : nullptr);
+  unsigned long long h[2] = {0, 0};
+  if (st == KC_OK) {
+    cudaError_t e = cudaMemcpyAsync(h, d_out, sizeof(h), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = kc::cuda_fail(e, "count readback", __FILE__, __LINE__);
+  }
+  cudaFreeAsync(d_out, s);
+  out->lo = h[0];
+  out->hi = h[1];
+  return st;
+}
+
+kc_status kc_kcore(kc_graph* g, uint32_t* core, uint32_t* max_core) {
+  if (!g) return fail(KC_ERR_INVALID_ARG, "graph is NULL");
+  kc::CtxLock lock(g->ctx);
+  KC_TRY(kc::peel_graph(g));
+  if (core && g->n) {
+    KC_CUDA(cudaMemcpyAsync(core, g->level, sizeof(uint32_t) * g->n, cudaMemcpyDeviceToHost, g->ctx->stream));
+    KC_CUDA(cudaStreamSynchronize(g->ctx->stream));
+  }
+  if (max_core) *max_core = g->max_core;
+  return KC_OK;
+}
+
+kc_status kc_truss_support(kc_graph* g, uint32_t* support) {
+  if (!g || (g->m && !support)) return fail(KC_ERR_INVALID_ARG, "NULL argument");
+  kc::CtxLock lock(g->ctx);
+  cudaStream_t s = g->ctx->stream;
+  uint32_t* d = nullptr;
+  KC_CUDA(cudaMallocAsync(&d, sizeof(uint32_t) * std::max<uint64_t>(1, g->m), s));
+  kc_status st = kc::truss_support(g, d);
+  if (st == KC_OK && g->m) {
+    cudaError_t e = cudaMemcpyAsync(support, d, sizeof(uint32_t) * g->m, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = kc::cuda_fail(e, "support readback", __FILE__, __LINE__);
+  }
+  cudaFreeAsync(d, s);
+  return st;
+}
+
+uint64_t kc_footprint_bytes(uint32_t n, uint64_t E, uint32_t max_out) {
+  // Resident graph: symmetric CSR (4(n+1) + 8m), rank maps (8n), DAG
+  // (4(n+1) + 4m), edge rows (4m), peel arrays (8n); build temporaries peak
+  // at about 16E + 16n; counting adds the unit queue (8 max(n, m)) and the
+  // per-group scratch of the largest class (bounded by 24 GiB).
+  const uint64_t m = E;
+  uint64_t resident = 4ull * (n + 1) + 8ull * m + 8ull * n + 4ull * (n + 1) + 4ull * m + 4ull * m + 8ull * n;
+  uint64_t build = 16ull * E + 16ull * n;
+  const uint64_t W = (max_out + 31) / 32;
+  uint64_t scratch = max_out > 1024 ? std::min<uint64_t>(24ull << 30, 148ull * 4 * max_out * W) : 64ull << 20;
+  uint64_t queue = 8ull * std::max<uint64_t>(n, m);
+  return resident + std::max(build, queue + scratch);
+}
+
+}  // extern "C"

@@ -1,0 +1,84 @@
+// Internal structures of the engine: the context, the device-resident graph
+// and the stage entry points that the C ABI (engine.cu) strings together.
+#pragma once
+#include <cstdint>
+#include <mutex>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/kc.h"
+#include "host_common.h"
+
+struct kc_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int sms = 148;
+  int max_smem_optin = 227 * 1024;
+  uint64_t spin_budget = 0;
+  uint64_t total_mem = 0;
+  std::mutex mu;  // one call at a time per context
+  // exact binomial table C(r, c) as (lo, hi) pairs, rows [0, brows], cols [0, bcols]
+  unsigned long long* d_binom = nullptr;
+  uint32_t brows = 0, bcols = 0;
+};
+
+struct kc_graph {
+  kc_ctx* ctx = nullptr;
+  uint32_t n = 0;
+  uint64_t m = 0;            // undirected edges
+  uint32_t max_deg = 0;
+  uint32_t* rp = nullptr;    // symmetric CSR, sorted rows, no duplicates / self-loops
+  uint32_t* col = nullptr;
+  // orientation (rank labels: vertex v has label rank[v]; u -> w iff rank[u] < rank[w])
+  int oriented = -1;         // -1 none, else kc_orientation
+  uint32_t* rank = nullptr;  // original id -> rank
+  uint32_t* inv = nullptr;   // rank -> original id
+  uint32_t* drp = nullptr;   // DAG row pointer, rank labels [n+1]
+  uint32_t* dcol = nullptr;  // DAG columns (ranks), sorted per row [m]
+  uint32_t* erow = nullptr;  // source rank of every DAG edge [m] (edge units)
+  uint32_t max_out = 0;
+  // degeneracy peel
+  uint32_t* prio = nullptr;  // reference-compatible peel priority (original ids)
+  uint32_t* level = nullptr; // peel level = core number (original ids)
+  uint32_t max_core = 0;
+  uint32_t* vgraph = nullptr; // batch: graph of every rank label (null for single graphs)
+  uint64_t bytes = 0;
+};
+
+namespace kc {
+
+// A device allocation tracked against the graph's byte count.
+kc_status dev_alloc(kc_graph* g, void** p, size_t bytes);
+void dev_free(kc_graph* g, void* p);
+
+// ---- stages (csr.cu, orient.cu, count.cu) ----
+// Builds the symmetric CSR from device edge arrays; n == 0 infers n.
+kc_status build_csr(kc_graph* g, const uint32_t* d_src, const uint32_t* d_dst, uint64_t n_edges,
+                    uint32_t n_nodes);
+kc_status orient_graph(kc_graph* g, uint32_t orientation);
+kc_status ensure_edge_rows(kc_graph* g);
+kc_status peel_graph(kc_graph* g);  // fills prio / level / max_core
+
+struct CountRequest {
+  uint32_t k;
+  uint32_t mode, unit, part, encoding, flags;
+  // batch: per-graph k (device, indexed by vgraph) and per-graph output
+  const uint32_t* d_graph_k = nullptr;
+  uint32_t n_graphs = 1;
+  uint32_t k_max = 0;
+};
+
+// Runs the counting stage; d_out holds n_graphs (lo, hi) pairs and must be zeroed.
+kc_status count_graph(kc_graph* g, const CountRequest& req, unsigned long long* d_out,
+                      kc_count_stats* stats);
+
+kc_status truss_support(kc_graph* g, uint32_t* d_support);
+
+// Exact binomial table on the device, grown on demand.
+kc_status ensure_binom(kc_ctx* ctx, uint32_t rows, uint32_t cols);
+
+// Autotuner: the kc_params a graph of this shape runs best with.
+kc_params autotune(uint32_t n, uint64_t m, uint32_t max_out, uint32_t k, uint32_t max_core);
+
+}  // namespace kc

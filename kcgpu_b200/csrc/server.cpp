@@ -1,0 +1,343 @@
+// Continuous-batching request server for clique-count queries.
+//
+// No counterpart in the reference (one graph per process, results printed).
+// Requests (a resident graph + k, or a one-shot edge list + k) enter a FIFO.
+// W worker threads, each with its own context and CUDA stream, take the head
+// of the queue as soon as (a) a worker is free and (b) the request's projected
+// device footprint fits in the HBM budget next to the resident graphs and the
+// requests already on the device. Requests therefore start while others are
+// still running, and their kernels overlap on the device through the workers'
+// streams. Results are exact integers, so a request's count is the same alone
+// and in any mix.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "engine.h"
+#include "host_common.h"
+
+namespace {
+
+struct Resident {
+  kc_graph* g = nullptr;
+  uint64_t bytes = 0;
+  kc_graph_info info{};
+  std::mutex mu;  // one request at a time per resident graph
+  ~Resident() {
+    if (g) kc_graph_destroy(g);
+  }
+};
+
+struct Request {
+  uint64_t ticket = 0;
+  uint64_t graph_id = 0;  // 0: one-shot
+  std::vector<uint32_t> src, dst;
+  uint32_t n = 0;
+  uint32_t k = 0;
+  uint64_t footprint = 0;
+  bool running = false, done = false;
+  kc_request_result res{};
+};
+
+}  // namespace
+
+struct kc_server {
+  kc_ctx* base = nullptr;
+  kc_server_opts opts{};
+  uint64_t budget = 0;
+  std::vector<kc_ctx*> wctx;
+  std::vector<std::thread> workers;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<std::shared_ptr<Request>> queue;
+  std::unordered_map<uint64_t, std::shared_ptr<Request>> reqs;
+  std::unordered_map<uint64_t, std::shared_ptr<Resident>> graphs;
+  uint64_t next_ticket = 1, next_graph = 1;
+  uint64_t inflight_bytes = 0, resident_bytes = 0;
+  uint32_t rr = 0;
+  bool stop = false;
+  std::chrono::steady_clock::time_point t0;
+
+  double ms() const {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+};
+
+namespace {
+
+kc_params choose(const kc_server* s, const kc_graph_info& inf, uint32_t k) {
+  kc_params p;
+  if (s->opts.autotune) {
+    p = kc::autotune(inf.n, inf.m, inf.max_out_degree, k, inf.max_core);
+  } else {
+    p = s->opts.fixed;
+    if (p.part == 0) p.part = 8;
+  }
+  p.k = k;
+  p.flags = 0;
+  if (k <= 2) p.unit = KC_UNIT_NODE;
+  return p;
+}
+
+void execute(kc_server* s, kc_ctx* ctx, Request& r) {
+  kc_u128 out{0, 0};
+  kc_status st = KC_OK;
+  if (r.graph_id) {
+    std::shared_ptr<Resident> res;
+    {
+      std::lock_guard<std::mutex> l(s->mu);
+      auto it = s->graphs.find(r.graph_id);
+      if (it != s->graphs.end()) res = it->second;
+    }
+    if (!res) {
+      st = kc::fail(KC_ERR_INVALID_ARG, "graph %llu is not resident", (unsigned long long)r.graph_id);
+    } else {
+      std::lock_guard<std::mutex> gl(res->mu);
+      kc_params p = choose(s, res->info, r.k);
+      r.res.params = p;
+      st = kc_count(res->g, &p, &out, nullptr);
+    }
+  } else {
+    kc_graph* g = nullptr;
+    st = kc_graph_from_edges(ctx, r.src.data(), r.dst.data(), r.src.size(), r.n, &g);
+    if (st == KC_OK) st = kc_orient(g, s->opts.orientation);
+    if (st == KC_OK) {
+      kc_graph_info inf;
+      kc_graph_get_info(g, &inf);
+      kc_params p = choose(s, inf, r.k);
+      r.res.params = p;
+      st = kc_count(g, &p, &out, nullptr);
+    }
+    if (g) kc_graph_destroy(g);
+    std::vector<uint32_t>().swap(r.src);
+    std::vector<uint32_t>().swap(r.dst);
+  }
+  r.res.count = out;
+  r.res.status = st;
+}
+
+void worker_main(kc_server* s, size_t wi) {
+  kc_ctx* ctx = s->wctx[wi];
+  for (;;) {
+    std::shared_ptr<Request> r;
+    {
+      std::unique_lock<std::mutex> l(s->mu);
+      s->cv_work.wait(l, [&]() {
+        if (s->stop) return true;
+        if (s->queue.empty()) return false;
+        const uint64_t fp = s->queue.front()->footprint;
+        return s->inflight_bytes == 0 || s->resident_bytes + s->inflight_bytes + fp <= s->budget;
+      });
+      if (s->stop) return;
+      r = s->queue.front();
+      s->queue.pop_front();
+      s->inflight_bytes += r->footprint;
+      r->running = true;
+      r->res.start_ms = s->ms();
+    }
+    execute(s, ctx, *r);
+    {
+      std::lock_guard<std::mutex> l(s->mu);
+      s->inflight_bytes -= r->footprint;
+      r->running = false;
+      r->done = true;
+      r->res.done_ms = s->ms();
+    }
+    s->cv_done.notify_all();
+    s->cv_work.notify_all();
+  }
+}
+
+kc_status enqueue(kc_server* s, std::shared_ptr<Request> r, uint64_t* ticket) {
+  {
+    std::lock_guard<std::mutex> l(s->mu);
+    if (r->footprint + s->resident_bytes > s->budget)
+      return kc::fail(KC_ERR_ADMISSION, "request needs %llu bytes; budget %llu with %llu resident",
+                      (unsigned long long)r->footprint, (unsigned long long)s->budget,
+                      (unsigned long long)s->resident_bytes);
+    r->ticket = s->next_ticket++;
+    r->res.submit_ms = s->ms();
+    r->res.k = r->k;
+    r->res.graph_id = r->graph_id;
+    r->res.status = KC_ERR_BUSY;
+    s->reqs[r->ticket] = r;
+    s->queue.push_back(r);
+    *ticket = r->ticket;
+  }
+  s->cv_work.notify_one();
+  return KC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+kc_status kc_server_create(kc_ctx* ctx, const kc_server_opts* opts, kc_server** out) {
+  kc::clear_error();
+  if (!ctx || !out) return kc::fail(KC_ERR_INVALID_ARG, "NULL argument");
+  *out = nullptr;
+  kc_server* s = new (std::nothrow) kc_server();
+  if (!s) return kc::fail(KC_ERR_OOM, "host allocation failed");
+  s->base = ctx;
+  if (opts) s->opts = *opts;
+  else {
+    std::memset(&s->opts, 0, sizeof(s->opts));
+    s->opts.autotune = 1;
+  }
+  if (s->opts.orientation > KC_ORIENT_DEGEN) {
+    delete s;
+    return kc::fail(KC_ERR_INVALID_ARG, "unknown orientation");
+  }
+  const uint64_t dev_total = ctx->total_mem ? ctx->total_mem : (180ull << 30);
+  s->budget = s->opts.hbm_budget_bytes ? s->opts.hbm_budget_bytes : std::min<uint64_t>(180ull * 1000000000ull, dev_total);
+  const uint32_t nw = std::max<uint32_t>(1, s->opts.streams ? s->opts.streams : (s->opts.max_inflight ? s->opts.max_inflight : 4));
+  s->t0 = std::chrono::steady_clock::now();
+  for (uint32_t i = 0; i < nw; ++i) {
+    kc_ctx* w = nullptr;
+    kc_status st = kc_ctx_create(ctx->device, &w);
+    if (st != KC_OK) {
+      for (auto* c : s->wctx) kc_ctx_destroy(c);
+      delete s;
+      return st;
+    }
+    s->wctx.push_back(w);
+  }
+  for (uint32_t i = 0; i < nw; ++i) s->workers.emplace_back(worker_main, s, (size_t)i);
+  *out = s;
+  return KC_OK;
+}
+
+kc_status kc_server_destroy(kc_server* s) {
+  if (!s) return KC_OK;
+  {
+    std::lock_guard<std::mutex> l(s->mu);
+    s->stop = true;
+    for (auto& r : s->queue) {
+      r->done = true;
+      r->res.status = KC_ERR_CANCELLED;
+    }
+    s->queue.clear();
+  }
+  s->cv_work.notify_all();
+  s->cv_done.notify_all();
+  for (auto& t : s->workers) t.join();
+  s->graphs.clear();
+  s->reqs.clear();
+  for (auto* c : s->wctx) kc_ctx_destroy(c);
+  delete s;
+  return KC_OK;
+}
+
+kc_status kc_server_put_graph(kc_server* s, const uint32_t* src, const uint32_t* dst, uint64_t n_edges,
+                              uint32_t n_nodes, uint64_t* graph_id) {
+  if (!s || !graph_id || (n_edges && (!src || !dst))) return kc::fail(KC_ERR_INVALID_ARG, "NULL argument");
+  const uint64_t fp = kc_footprint_bytes(n_nodes, n_edges, 0);
+  kc_ctx* owner;
+  {
+    std::lock_guard<std::mutex> l(s->mu);
+    if (s->resident_bytes + fp > s->budget)
+      return kc::fail(KC_ERR_ADMISSION, "graph needs %llu bytes; %llu of %llu already resident",
+                      (unsigned long long)fp, (unsigned long long)s->resident_bytes, (unsigned long long)s->budget);
+    owner = s->wctx[s->rr++ % s->wctx.size()];
+  }
+  auto res = std::make_shared<Resident>();
+  KC_TRY(kc_graph_from_edges(owner, src, dst, n_edges, n_nodes, &res->g));
+  KC_TRY(kc_orient(res->g, s->opts.orientation));
+  kc_graph_get_info(res->g, &res->info);
+  res->bytes = res->info.device_bytes;
+  std::lock_guard<std::mutex> l(s->mu);
+  const uint64_t id = s->next_graph++;
+  s->graphs[id] = res;
+  s->resident_bytes += res->bytes;
+  *graph_id = id;
+  return KC_OK;
+}
+
+kc_status kc_server_drop_graph(kc_server* s, uint64_t graph_id) {
+  if (!s) return kc::fail(KC_ERR_INVALID_ARG, "server is NULL");
+  std::shared_ptr<Resident> res;
+  {
+    std::lock_guard<std::mutex> l(s->mu);
+    auto it = s->graphs.find(graph_id);
+    if (it == s->graphs.end()) return kc::fail(KC_ERR_INVALID_ARG, "graph %llu is not resident", (unsigned long long)graph_id);
+    res = it->second;
+    s->resident_bytes -= res->bytes;
+    s->graphs.erase(it);
+  }
+  return KC_OK;  // freed when the last request using it finishes
+}
+
+kc_status kc_server_submit(kc_server* s, uint64_t graph_id, uint32_t k, uint64_t* ticket) {
+  if (!s || !ticket) return kc::fail(KC_ERR_INVALID_ARG, "NULL argument");
+  if (k < 1) return kc::fail(KC_ERR_INVALID_ARG, "k must be >= 1");
+  auto r = std::make_shared<Request>();
+  {
+    std::lock_guard<std::mutex> l(s->mu);
+    auto it = s->graphs.find(graph_id);
+    if (it == s->graphs.end()) return kc::fail(KC_ERR_INVALID_ARG, "graph %llu is not resident", (unsigned long long)graph_id);
+    const auto& inf = it->second->info;
+    // counting scratch only: the graph itself is already resident
+    r->footprint = kc_footprint_bytes(inf.n, inf.m, inf.max_out_degree) - inf.device_bytes / 2;
+  }
+  r->graph_id = graph_id;
+  r->k = k;
+  return enqueue(s, r, ticket);
+}
+
+kc_status kc_server_submit_edges(kc_server* s, const uint32_t* src, const uint32_t* dst, uint64_t n_edges,
+                                 uint32_t n_nodes, uint32_t k, uint64_t* ticket) {
+  if (!s || !ticket || (n_edges && (!src || !dst))) return kc::fail(KC_ERR_INVALID_ARG, "NULL argument");
+  if (k < 1) return kc::fail(KC_ERR_INVALID_ARG, "k must be >= 1");
+  auto r = std::make_shared<Request>();
+  r->src.assign(src, src + n_edges);
+  r->dst.assign(dst, dst + n_edges);
+  r->n = n_nodes;
+  r->k = k;
+  r->footprint = kc_footprint_bytes(n_nodes, n_edges, 0);
+  return enqueue(s, r, ticket);
+}
+
+kc_status kc_server_cancel(kc_server* s, uint64_t ticket) {
+  if (!s) return kc::fail(KC_ERR_INVALID_ARG, "server is NULL");
+  std::lock_guard<std::mutex> l(s->mu);
+  auto it = s->reqs.find(ticket);
+  if (it == s->reqs.end()) return kc::fail(KC_ERR_INVALID_ARG, "unknown ticket %llu", (unsigned long long)ticket);
+  auto r = it->second;
+  if (r->done) return KC_OK;
+  if (r->running) return kc::fail(KC_ERR_BUSY, "request %llu is already running", (unsigned long long)ticket);
+  s->queue.erase(std::remove(s->queue.begin(), s->queue.end(), r), s->queue.end());
+  r->done = true;
+  r->res.status = KC_ERR_CANCELLED;
+  r->res.done_ms = s->ms();
+  s->cv_done.notify_all();
+  return KC_OK;
+}
+
+kc_status kc_server_wait(kc_server* s, uint64_t ticket, int64_t wait_ms, kc_request_result* out) {
+  if (!s || !out) return kc::fail(KC_ERR_INVALID_ARG, "NULL argument");
+  std::unique_lock<std::mutex> l(s->mu);
+  auto it = s->reqs.find(ticket);
+  if (it == s->reqs.end()) return kc::fail(KC_ERR_INVALID_ARG, "unknown ticket %llu", (unsigned long long)ticket);
+  auto r = it->second;
+  if (wait_ms < 0) s->cv_done.wait(l, [&]() { return r->done; });
+  else if (wait_ms > 0) s->cv_done.wait_for(l, std::chrono::milliseconds(wait_ms), [&]() { return r->done; });
+  if (!r->done) return kc::fail(KC_ERR_BUSY, "request %llu not finished", (unsigned long long)ticket);
+  *out = r->res;
+  s->reqs.erase(ticket);
+  return r->res.status == KC_OK ? KC_OK
+                                : kc::fail((kc_status)r->res.status, "request %llu failed: %s", (unsigned long long)ticket,
+                                           kc_status_string((kc_status)r->res.status));
+}
+
+}  // extern "C"
