@@ -157,6 +157,21 @@ kc_status kc_kcore(kc_graph* g, uint32_t* core, uint32_t* max_core);
 /* sup(u,v) = |N(u) ∩ N(v)| for every undirected edge u<v, in the row-major
  * order of the upper triangle of the symmetric CSR (m entries, host). */
 kc_status kc_truss_support(kc_graph* g, uint32_t* support);
+/* No counterpart in the reference. The same supports as kc_truss_support for
+ * callers that may not allocate device memory during the call (a plugin whose
+ * host runtime owns all device memory, a latency-critical stream that must not
+ * be stalled by cudaMalloc/cudaFree, a pipeline that reserves memory up
+ * front). Inputs and output are device pointers on the current device: a
+ * symmetric CSR with sorted, duplicate-free rows (d_row_ptr[n_nodes+1],
+ * d_col_ind) and d_support with room for one value per undirected edge. Work
+ * is enqueued on `stream` (a cudaStream_t, NULL = default stream) and nothing
+ * is allocated: the only scratch is a fixed 1 MiB array inside the library, so
+ * n_nodes may be at most 262,144 (larger graphs return KC_ERR_INVALID_ARG).
+ * Calls on one device share that array: calls that overlap on the GPU race and
+ * must be ordered by the caller. The first call on each device looks up the
+ * array's address; make it before any stream capture begins. */
+kc_status kc_truss_support_noalloc(const uint32_t* d_row_ptr, const uint32_t* d_col_ind,
+                                   uint32_t n_nodes, uint32_t* d_support, void* stream);
 
 /* ---- batched counting ------------------------------------------------ */
 /* One graph of a batch: an edge list in host memory plus its own k. */

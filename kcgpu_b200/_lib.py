@@ -82,6 +82,7 @@ SIGNATURES = {
     "kc_parse_spec": (i32, [C.c_char_p, P(KcParams)]),
     "kc_kcore": (i32, [C.c_void_p, P(u32), P(u32)]),
     "kc_truss_support": (i32, [C.c_void_p, P(u32)]),
+    "kc_truss_support_noalloc": (i32, [C.c_void_p, C.c_void_p, u32, C.c_void_p, C.c_void_p]),
     "kc_batch_count": (i32, [C.c_void_p, P(KcBatchGraph), u32, P(KcBatchOpts), P(KcU128), P(KcParams),
                              P(KcBatchStats)]),
     "kc_batch_count_packed": (i32, [C.c_void_p, P(u32), P(u32), P(u64), P(u32), P(u32), u32, P(KcBatchOpts),
