@@ -144,6 +144,13 @@ def make_batch(kc, n_graphs: int, seed: int):
     return el, s, d, off, nn, kk, fam
 
 
+def cpu_modes(kk, fam):
+    """The CPU counter's algorithm per graph: the Pivoter for graphs that hold
+    a planted clique or ask for k >= 9, orientation listing for the rest (the
+    faster of the two on the CPU for each family)."""
+    return [1 if (int(k) >= 9 or int(f) == 2) else 0 for k, f in zip(kk, fam)]
+
+
 def cpu_oracle_sample(s, d, off, nn, kk, modes, budget_s: float):
     """The CPU oracle on graphs 0, 1, ... until budget_s elapses; returns
     (graphs done, seconds, counts)."""
@@ -171,7 +178,7 @@ def run_reference(args, world, rank, local, pg):
     from oracle.oracle import max_threads
 
     el, s, d, off, nn, kk, fam = make_batch(kc, args.graphs, args.seed)
-    modes = [1 if (k >= 9 or f == 2) else 0 for k, f in zip(kk, fam)]
+    modes = cpu_modes(kk, fam)
     # size one step to ~12 s of CPU work on this host
     probe, t_probe, _ = cpu_oracle_sample(s, d, off, nn, kk, modes, 3.0)
     per_graph = t_probe / max(1, probe)
@@ -236,12 +243,15 @@ def main():
     l0 = L.kc_kernel_launches()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     stage = {"ms_h2d": [], "ms_build": [], "ms_count": []}
+    trav = {"tree_nodes": 0, "word_ops": 0, "gather_bytes": 0, "heavy_units": 0}
     for i in range(args.steps):
         evs[i][0].record(stream)
         counts, choice, st = run_device()
         evs[i][1].record(stream)
         for key in stage:
             stage[key].append(st[key])
+        for key in trav:
+            trav[key] += st[key]
     torch.cuda.synchronize()
     launches = (L.kc_kernel_launches() - l0) // max(1, args.steps)
     clk = clocks.stop()
@@ -267,7 +277,7 @@ def main():
     total_cliques = sum(counts)
     out = None
     if rank == 0:
-        modes = [c["mode"] for c in choice]
+        modes = cpu_modes(kk, fam)
         # plain path: one graph per call on a sample of the same batch
         P = min(args.plain_sample, G)
         t0 = time.perf_counter()
@@ -294,6 +304,29 @@ def main():
                    "bitexact": bitexact_cpu}
         h2d = 8 * E + 8 * (G + 1) + 8 * G
         ms_count = sum(stage["ms_count"]) / len(stage["ms_count"])
+        # Roofline of the dominant stage, the counting launch (k_count_bitmap):
+        # its algorithmic HBM bytes are the adjacency lists gathered to build
+        # the induced subgraphs (measured by the kernels' counters); the
+        # traversal itself runs from shared memory, so the word-op figure is
+        # given beside it against the POPC issue rate (16 per SM per clock).
+        peaks = {}
+        try:
+            peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        except (OSError, ValueError):
+            pass
+        hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+        steps = max(1, args.steps)
+        gb_s = (trav["gather_bytes"] / steps) / (ms_count / 1e3) / 1e9
+        sm_mhz = (clk.get("sm_mhz") or 1965.0)
+        popc_peak = 16 * 148 * sm_mhz * 1e6
+        wops = (trav["word_ops"] / steps) / (ms_count / 1e3)
+        roofline = {"bound": "hbm", "kernel": "k_count_bitmap (all counting launches of a step)",
+                    "achieved": gb_s, "peak": hbm_peak, "unit": "GB/s", "frac": gb_s / hbm_peak,
+                    "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s",
+                    "algorithmic_bytes_per_step": trav["gather_bytes"] / steps, "traffic": None,
+                    "word_ops_per_s": wops, "popc_peak_per_s": popc_peak, "popc_frac": wops / popc_peak,
+                    "tree_nodes_per_step": trav["tree_nodes"] / steps,
+                    "heavy_units_per_step": trav["heavy_units"] / steps}
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_step, "higher_is_better": True, "scaling": "weak",
@@ -312,7 +345,7 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clk,
             "cpu_baseline": cpu,
-            "roofline": None,
+            "roofline": roofline,
         }
     if rank == 0:
         print(json.dumps(out), flush=True)

@@ -60,7 +60,11 @@ typedef enum kc_status {
 } kc_status;
 
 typedef enum kc_orientation { KC_ORIENT_DEGREE = 0, KC_ORIENT_DEGEN = 1 } kc_orientation;
-typedef enum kc_mode { KC_MODE_ORIENT = 0, KC_MODE_PIVOT = 1 } kc_mode;
+/* KC_MODE_ORIENT and KC_MODE_PIVOT are the reference's two algorithms (-q o|p).
+ * KC_MODE_AUTO (an engine extension) lists each small unit by orientation and
+ * switches a unit to pivoting when its traversal outgrows a fixed budget, and
+ * pivots every large unit; the count is the same in every mode. */
+typedef enum kc_mode { KC_MODE_ORIENT = 0, KC_MODE_PIVOT = 1, KC_MODE_AUTO = 2 } kc_mode;
 typedef enum kc_unit { KC_UNIT_NODE = 0, KC_UNIT_EDGE = 1 } kc_unit;
 typedef enum kc_encoding { KC_ENC_BITMAP = 0, KC_ENC_LIST = 1 } kc_encoding;
 
@@ -188,7 +192,7 @@ typedef struct kc_batch_opts {
   uint32_t autotune;      /* 1 = choose mode/unit/part/encoding per graph */
   kc_params fixed;        /* used when autotune == 0 (k ignored) */
   uint32_t use_graph;     /* 1 = replay the counting stage as a captured CUDA graph */
-  uint32_t reserved;
+  uint32_t flags;         /* KC_FLAG_STATS: fill the traversal counters below */
 } kc_batch_opts;
 
 typedef struct kc_batch_stats {
@@ -199,6 +203,10 @@ typedef struct kc_batch_stats {
   uint64_t units;
   uint32_t kernels;
   uint32_t n_graphs;
+  uint64_t tree_nodes;    /* with KC_FLAG_STATS: traversal nodes expanded */
+  uint64_t word_ops;      /* with KC_FLAG_STATS: 32-bit AND+POPC word operations */
+  uint64_t gather_bytes;  /* with KC_FLAG_STATS: adjacency bytes read for induced subgraphs */
+  uint64_t heavy_units;   /* units handed from a warp to the CTA-wide heavy pass */
 } kc_batch_stats;
 
 /* Counts every graph of the batch; counts[i] receives graph i's count and

@@ -25,7 +25,7 @@ __all__ = ["Context", "Graph", "KCError", "SingleGPU_Kclique", "parse_spec", "MO
            "ORIENTATIONS", "EdgeList", "gen_er", "gen_rmat", "gen_chung_lu", "gen_sbm", "gen_batch",
            "batch_count", "footprint_bytes", "lib"]
 
-MODES = {"orient": 0, "orientation": 0, "o": 0, "pivot": 1, "pivoting": 1, "p": 1}
+MODES = {"orient": 0, "orientation": 0, "o": 0, "pivot": 1, "pivoting": 1, "p": 1, "auto": 2}
 UNITS = {"node": 0, "edge": 1}
 ENCODINGS = {"bitmap": 0, "binary": 0, "b": 0, "list": 1, "n": 1}
 ORIENTATIONS = {"degree": 0, "degen": 1, "degeneracy": 1}
@@ -366,6 +366,7 @@ def batch_count(ctx: Context, src, dst, edge_off, n_nodes, ks, orientation="degr
     opts.orientation = ORIENTATIONS[orientation] if isinstance(orientation, str) else int(orientation)
     opts.autotune = 1 if autotune else 0
     opts.use_graph = 1 if use_graph else 0
+    opts.flags = 1 if return_stats else 0
     if fixed:
         opts.fixed.mode = MODES.get(fixed.get("mode", "orient"), 0) if isinstance(fixed.get("mode"), str) else int(fixed.get("mode", 0))
         opts.fixed.unit = UNITS.get(fixed.get("unit", "node"), 0) if isinstance(fixed.get("unit"), str) else int(fixed.get("unit", 0))

@@ -42,12 +42,13 @@ class KcBatchGraph(C.Structure):
 
 class KcBatchOpts(C.Structure):
     _fields_ = [("orientation", u32), ("autotune", u32), ("fixed", KcParams), ("use_graph", u32),
-                ("reserved", u32)]
+                ("flags", u32)]
 
 
 class KcBatchStats(C.Structure):
     _fields_ = [("ms_total", C.c_double), ("ms_h2d", C.c_double), ("ms_build", C.c_double),
-                ("ms_count", C.c_double), ("units", u64), ("kernels", u32), ("n_graphs", u32)]
+                ("ms_count", C.c_double), ("units", u64), ("kernels", u32), ("n_graphs", u32),
+                ("tree_nodes", u64), ("word_ops", u64), ("gather_bytes", u64), ("heavy_units", u64)]
 
 
 class KcServerOpts(C.Structure):

@@ -191,7 +191,7 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool 
       p.k = ks[g];
       if (ks[g] <= 2) p.unit = KC_UNIT_NODE;  // an edge unit cannot count 1-cliques
       p.flags = 0;
-      if (p.mode > 1 || p.unit > 1 || p.encoding > 1 || p.part == 0 || p.part > 32 || (p.part & (p.part - 1))) {
+      if (p.mode > KC_MODE_AUTO || p.unit > 1 || p.encoding > 1 || p.part > 32 || (p.part & (p.part - 1))) {
         st = fail(KC_ERR_INVALID_ARG, "bad fixed parameters for the batch");
         break;
       }
@@ -227,7 +227,7 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool 
       req.unit = kv.first.unit;
       req.part = kv.first.part;
       req.encoding = kv.first.enc;
-      req.flags = 0;
+      req.flags = opts ? (opts->flags & KC_FLAG_STATS) : 0u;
       req.d_graph_k = dk;
       req.n_graphs = G;
       req.k_max = kmax;
@@ -267,15 +267,20 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool 
       cudaEventRecord(e4, s);
     }
   }
+  unsigned long long trav[3] = {0, 0, 0};
+  uint64_t heavy_units = 0;
   if (st == KC_OK) {
     bool deep = false;
     for (auto& pl : plans) {
-      uint32_t err = count_error(pl, s, nullptr);
+      unsigned long long sv[3] = {0, 0, 0};
+      uint32_t err = count_error(pl, s, sv);
       if (err == DEV_ERR_STACK) deep = true;
       else if (err) st = fail(KC_ERR_INTERNAL, "batched counting reported device error %u", err);
+      for (int q = 0; q < 3; ++q) trav[q] += sv[q];
+      heavy_units += count_heavy(pl, s);
       units += count_units(pl, s);
       kernels += 5;
-      for (int c = 0; c < kNumClasses; ++c) kernels += pl.active[c] ? 1 : 0;
+      for (int c = 0; c <= kNumClasses; ++c) kernels += pl.active[c] ? 1 : 0;
     }
     if (st == KC_OK && deep) {
       // a clique tree deeper than the fast stack: rerun every pass with full depth
@@ -315,6 +320,10 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool 
     stats->units = units;
     stats->kernels = kernels;
     stats->n_graphs = G;
+    stats->tree_nodes = trav[0];
+    stats->word_ops = trav[1];
+    stats->gather_bytes = trav[2];
+    stats->heavy_units = heavy_units;
   }
   if (cge) cudaGraphExecDestroy(cge);
   if (cg) cudaGraphDestroy(cg);

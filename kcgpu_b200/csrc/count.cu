@@ -140,11 +140,11 @@ kc_status ensure_binom(kc_ctx* ctx, uint32_t rows, uint32_t cols) {
 
 void count_release(CountPlan* pl) {
   cudaStream_t s = pl->g->ctx->stream;
-  for (int c = 0; c < kNumClasses; ++c) release_launch(pl->launches[c], s);
-  void* ps[] = {pl->size, pl->hist, pl->rev, pl->queue, pl->scratch};
+  for (int c = 0; c <= kNumClasses; ++c) release_launch(pl->launches[c], s);
+  void* ps[] = {pl->size, pl->hist, pl->rev, pl->queue, pl->scratch, pl->heavy};
   for (void* p : ps)
     if (p) cudaFreeAsync(p, s);
-  pl->size = pl->hist = pl->rev = pl->queue = pl->scratch = nullptr;
+  pl->size = pl->hist = pl->rev = pl->queue = pl->scratch = pl->heavy = nullptr;
 }
 
 // Allocates the queue and the class launches. No kernel runs; the plan can be
@@ -163,34 +163,50 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
   pl->max_size = g->max_out;
   if (pl->max_size >= 65535u)
     return fail(KC_ERR_INVALID_ARG, "largest out-degree %u exceeds the 65534 supported per unit", pl->max_size);
-  if (req.mode == KC_MODE_PIVOT) KC_TRY(ensure_binom(ctx, pl->max_size + 2, k_max + 1));
+  if (req.mode != KC_MODE_ORIENT) KC_TRY(ensure_binom(ctx, pl->max_size + 2, k_max + 1));
   const uint32_t nu = std::max<uint32_t>(1, pl->n_units);
   KC_CUDA(cudaMallocAsync(&pl->size, sizeof(uint32_t) * nu, s));
   KC_CUDA(cudaMallocAsync(&pl->queue, sizeof(uint32_t) * nu, s));
+  KC_CUDA(cudaMallocAsync(&pl->heavy, sizeof(uint32_t) * nu, s));
   KC_CUDA(cudaMallocAsync(&pl->hist, sizeof(uint32_t) * ((size_t)pl->max_size + 2), s));
   KC_CUDA(cudaMallocAsync(&pl->rev, sizeof(uint32_t) * ((size_t)pl->max_size + 2), s));
-  KC_CUDA(cudaMallocAsync(&pl->scratch, sizeof(uint32_t) * 64, s));
-  for (int c = 0; c < kNumClasses; ++c) {
-    if ((int64_t)pl->max_size <= kClasses[c].lo) continue;
+  KC_CUDA(cudaMallocAsync(&pl->scratch, sizeof(uint32_t) * kScratchWords, s));
+  // Per-launch algorithm: orientation or pivot as requested; KC_MODE_AUTO
+  // lists small units by orientation (cheap when their neighbourhood holds few
+  // cliques) and counts large units and over-budget units with the pivot.
+  const bool budget_ok = req.encoding == KC_ENC_BITMAP;
+  auto launch_mode = [&](bool warp_group, bool heavy_pass) -> uint32_t {
+    if (req.mode != KC_MODE_AUTO) return req.mode;
+    // orientation listing only where a budget can hand a clique-heavy unit
+    // on to the pivot; without one (list encoding) AUTO pivots everywhere
+    return (warp_group && !heavy_pass && budget_ok) ? (uint32_t)KC_MODE_ORIENT : (uint32_t)KC_MODE_PIVOT;
+  };
+  bool any_budget = false;
+  for (int c = 0; c <= kNumClasses; ++c) {
+    const bool heavy_pass = c == kNumClasses;
+    if (heavy_pass && !any_budget) continue;
+    if (!heavy_pass && (int64_t)pl->max_size <= kClasses[c].lo) continue;
+    const bool warp_group = !heavy_pass && kClasses[c].G == 32;
     LaunchPlan lp;
-    lp.mode = req.mode;
+    lp.mode = launch_mode(warp_group, heavy_pass);
     lp.encoding = req.encoding;
     lp.edge = pl->edge;
-    lp.dcap = (uint32_t)std::max<int64_t>(1, std::min<int64_t>(kClasses[c].hi, pl->max_size));
-    lp.G = kClasses[c].G;
-    lp.block = kClasses[c].block;
+    lp.dcap = heavy_pass ? std::max<uint32_t>(1, std::min<uint32_t>(kWarpClassMax, pl->max_size))
+                         : (uint32_t)std::max<int64_t>(1, std::min<int64_t>(kClasses[c].hi, pl->max_size));
+    lp.G = heavy_pass ? 256 : kClasses[c].G;
+    lp.block = heavy_pass ? 256 : kClasses[c].block;
     lp.force_global_bitmap = (c == 0);
     lp.k_max = k_max;
-    lp.part = req.part ? req.part : auto_part(req.mode, (lp.dcap + 31) / 32);
+    lp.part = req.part ? req.part : auto_part(lp.mode, (lp.dcap + 31) / 32);
     lp.depth_boost = depth_boost;
     CountParams p;
     std::memset(&p, 0, sizeof(p));
     p.rp = g->drp;
     p.col = g->dcol;
     p.erow = g->erow;
-    p.queue = pl->queue;
-    p.bounds = pl->scratch + 32;
-    p.cls = (uint32_t)c;
+    p.queue = heavy_pass ? pl->heavy : pl->queue;
+    p.bounds = pl->scratch + (heavy_pass ? kHeavyBounds : kClassBounds);
+    p.cls = heavy_pass ? 0u : (uint32_t)c;
     p.n_units_max = pl->n_units;
     p.edge_units = pl->edge ? 1 : 0;
     p.vgraph = g->vgraph;
@@ -200,8 +216,15 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
     p.binom = ctx->d_binom;
     p.binom_cols = ctx->bcols;
     p.ticket = pl->scratch + c;
-    p.err = pl->scratch + 8;
-    p.stats = (req.flags & KC_FLAG_STATS) ? reinterpret_cast<unsigned long long*>(pl->scratch + 16) : nullptr;
+    p.err = pl->scratch + kErrWord;
+    p.stats = (req.flags & KC_FLAG_STATS) ? reinterpret_cast<unsigned long long*>(pl->scratch + kStatsWords)
+                                          : nullptr;
+    if (warp_group && budget_ok) {
+      p.budget = kUnitBudget;
+      p.heavy = pl->heavy;
+      p.heavy_count = pl->scratch + kHeavyBounds + 1;
+      any_budget = true;
+    }
     KC_TRY(prepare_launch(ctx, lp, p, s, &pl->launches[c]));
     pl->active[c] = true;
   }
@@ -215,32 +238,40 @@ kc_status count_enqueue(const CountPlan& pl, cudaStream_t s) {
   const int sms = g->ctx->sms;
   const uint32_t M = pl.max_size;
   KC_CUDA(cudaMemsetAsync(pl.hist, 0, sizeof(uint32_t) * ((size_t)M + 2), s));
-  KC_CUDA(cudaMemsetAsync(pl.scratch, 0, sizeof(uint32_t) * 32, s));
+  KC_CUDA(cudaMemsetAsync(pl.scratch, 0, sizeof(uint32_t) * kScratchWords, s));
   const uint32_t gq = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((pl.n_units + 255) / 256, (uint64_t)sms * 16));
   if (pl.n_units)
     k_unit_sizes<<<gq, 256, 0, s>>>(g->drp, g->dcol, g->erow, pl.n_units, pl.edge ? 1 : 0, g->vgraph,
                                     pl.req.d_graph_k, pl.req.k, pl.size, pl.hist);
   k_reverse<<<(M + 1 + 255) / 256, 256, 0, s>>>(pl.hist, M + 1, pl.rev);
   KC_CUDA(prim::scan_exclusive_u32(pl.rev, pl.rev, M + 1, s));
-  k_class_bounds<<<1, 32, 0, s>>>(pl.rev, M, pl.scratch + 32);
+  k_class_bounds<<<1, 32, 0, s>>>(pl.rev, M, pl.scratch + kClassBounds);
   if (pl.n_units) k_unit_scatter<<<gq, 256, 0, s>>>(pl.size, pl.n_units, M, pl.rev, pl.queue);
   KC_CUDA(cudaGetLastError());
-  for (int c = 0; c < kNumClasses; ++c)
+  // class launches, then the heavy pass over the units they handed on
+  for (int c = 0; c <= kNumClasses; ++c)
     if (pl.active[c]) KC_TRY(enqueue_launch(pl.launches[c], s));
   return KC_OK;
 }
 
 uint32_t count_error(const CountPlan& pl, cudaStream_t s, unsigned long long* stats3) {
-  uint32_t h[64];
+  uint32_t h[kScratchWords];
   cudaMemcpyAsync(h, pl.scratch, sizeof(h), cudaMemcpyDeviceToHost, s);
   cudaStreamSynchronize(s);
-  if (stats3) std::memcpy(stats3, h + 16, 3 * sizeof(unsigned long long));
-  return h[8];
+  if (stats3) std::memcpy(stats3, h + kStatsWords, 3 * sizeof(unsigned long long));
+  return h[kErrWord];
+}
+
+uint32_t count_heavy(const CountPlan& pl, cudaStream_t s) {
+  uint32_t h = 0;
+  cudaMemcpyAsync(&h, pl.scratch + kHeavyBounds + 1, sizeof(h), cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  return h;
 }
 
 uint64_t count_units(const CountPlan& pl, cudaStream_t s) {
   uint32_t b[2 * kNumClasses];
-  cudaMemcpyAsync(b, pl.scratch + 32, sizeof(b), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(b, pl.scratch + kClassBounds, sizeof(b), cudaMemcpyDeviceToHost, s);
   cudaStreamSynchronize(s);
   uint64_t t = 0;
   for (int c = 0; c < kNumClasses; ++c) t += b[2 * c + 1];
@@ -270,11 +301,11 @@ kc_status count_graph(kc_graph* g, const CountRequest& req, unsigned long long* 
       err = count_error(pl, s, sv);
       units = count_units(pl, s);
       kernels = 5;
-      for (int c = 0; c < kNumClasses; ++c) kernels += pl.active[c] ? 1 : 0;
+      for (int c = 0; c <= kNumClasses; ++c) kernels += pl.active[c] ? 1 : 0;
     }
     count_release(&pl);
     if (st != KC_OK) break;
-    if (err == DEV_ERR_STACK && boost == 0 && req.mode == KC_MODE_PIVOT) {
+    if (err == DEV_ERR_STACK && boost == 0 && req.mode != KC_MODE_ORIENT) {
       // a clique tree deeper than the fast stack: rerun with the full depth
       KC_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long) * 2 * req.n_graphs, s));
       continue;

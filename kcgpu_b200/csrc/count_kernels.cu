@@ -90,15 +90,42 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
     acc = 0;
   };
 
+  // Work budget: a unit whose traversal exceeds p.budget nodes stops, drops
+  // its partial count and is appended to the heavy list, which a CTA-wide
+  // pass counts afterwards. Nodes are charged to hdr[4] in steps of 64 and
+  // hdr[5] flags the stop; each partition keeps the unit's count in uacc
+  // until the unit is known to have finished.
+  const bool budgeted = p.budget != 0;
+  unsigned __int128 uacc = 0;
+  uint32_t since_charge = 0;
+  auto over_budget = [&]() -> bool {  // partition-uniform
+    uint32_t stop = 0;
+    if (pt.plane == 0) {
+      stop = *(volatile uint32_t*)&hdr[5];
+      if (!stop && ++since_charge >= 64) {
+        since_charge = 0;
+        if (atomicAdd(&hdr[4], 64u) + 64u > p.budget) {
+          hdr[5] = 1u;
+          stop = 1u;
+        }
+      }
+    }
+    return __shfl_sync(pt.pmask, stop, pt.pbase) != 0u;
+  };
+
   for (;;) {
     if (gt == 0) {
       hdr[0] = atomicAdd(p.ticket, 1u);
       hdr[1] = 0;  // subtree ticket of this unit
+      hdr[4] = 0;  // nodes charged to this unit
+      hdr[5] = 0;  // unit over budget
     }
     gsync();
     const uint32_t ui = hdr[0];
     if (ui >= ucnt) break;
     const uint32_t unit = p.queue[ubeg + ui];
+    uacc = 0;
+    since_charge = 0;
     uint32_t src, d;
     if (!p.edge_units) {
       src = unit;
@@ -202,6 +229,7 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
       // ---- orientation traversal
       const uint32_t t = p.edge_units ? k - 2u : k - 1u;
       for (;;) {
+        if (budgeted && over_budget()) break;
         uint32_t j = 0;
         if (pt.plane == 0) j = atomicAdd(&hdr[1], 1u);
         j = __shfl_sync(pt.pmask, j, pt.pbase);
@@ -217,12 +245,13 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
         c = __reduce_add_sync(pt.pmask, c);
         st_nodes++;
         st_words += W - ws;
-        if (t == 2u) { acc += c; continue; }
+        if (t == 2u) { uacc += c; continue; }
         if (c < t - 1u) continue;
         if (pt.plane == 0) F0[W] = ws;
         __syncwarp(pt.pmask);
         int lv = 0;
         while (lv >= 0) {
+          if (budgeted && over_budget()) break;
           uint32_t* F = frames + (size_t)lv * p.fw;
           uint32_t wi = 0;
           const int vb = part_next_bit(F, F[W], W, pt, &wi);
@@ -244,7 +273,7 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
           st_nodes++;
           st_words += W - wi;
           if (rem == 1u) {
-            acc += cc;
+            uacc += cc;
           } else if (cc >= rem) {
             if (!store) {
               if (pt.plane == 0) set_error(p.err, DEV_ERR_STACK);
@@ -285,7 +314,7 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
         if (nc == 0u) {
           if (hold <= k && hold + drop >= k) {
             const unsigned long long* e = p.binom + 2ull * ((size_t)drop * (p.binom_cols + 1u) + (k - hold));
-            acc += ((unsigned __int128)e[1] << 64) | e[0];
+            uacc += ((unsigned __int128)e[1] << 64) | e[0];
           }
           return false;
         }
@@ -337,6 +366,7 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
       };
 
       for (;;) {
+        if (budgeted && over_budget()) break;
         uint32_t v = 0;
         if (pt.plane == 0) v = atomicAdd(&hdr[1], 1u);
         v = __shfl_sync(pt.pmask, v, pt.pbase);
@@ -351,6 +381,7 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
         if (!enter(F0, hold, drop)) continue;
         int lv = 0;
         while (lv >= 0) {
+          if (budgeted && over_budget()) break;
           uint32_t* F = frames + (size_t)lv * p.fw;
           uint32_t wi = 0;
           const int vb = part_next_bit(F + W, F[2 * W + 3], W, pt, &wi);
@@ -378,6 +409,13 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
           if (descend && enter(Fc, h2, d2)) ++lv;
         }
       }
+    }
+    gsync();
+    // commit the unit, or hand it to the heavy pass when it ran over budget
+    if (budgeted && hdr[5]) {
+      if (gt == 0) p.heavy[atomicAdd(p.heavy_count, 1u)] = unit;
+    } else {
+      acc += uacc;
     }
     gsync();
   }

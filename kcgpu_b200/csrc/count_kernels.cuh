@@ -39,6 +39,9 @@ struct CountParams {
   uint32_t* ticket;          // unit ticket (zeroed)
   uint32_t* err;             // device error word
   unsigned long long* stats; // [0] tree nodes [1] word-ops [2] gather bytes, or null
+  uint32_t budget;           // traversal nodes a unit may use before it is handed on (0 = no limit)
+  uint32_t* heavy;           // units over budget, counted again by the heavy pass
+  uint32_t* heavy_count;     // their number (atomic)
 };
 
 struct LaunchPlan {
@@ -71,8 +74,18 @@ kc_status prepare_launch_list(kc_ctx* ctx, const LaunchPlan& lp, const CountPara
 kc_status enqueue_launch(const PreparedLaunch& pl, cudaStream_t s);
 void release_launch(PreparedLaunch& pl, cudaStream_t s);
 
-// Unit-size classes of the persistent queue.
+// Unit-size classes of the persistent queue; launch kNumClasses is the heavy
+// pass (CTA per unit) over the warp-class units that ran over budget.
 constexpr int kNumClasses = 4;
+constexpr uint32_t kWarpClassMax = 128;   // largest unit a warp group takes
+constexpr uint32_t kUnitBudget = 8192;    // traversal nodes before a warp unit is handed on
+
+// Layout of a plan's scratch words (zeroed by every enqueue).
+constexpr uint32_t kScratchWords = 48;
+constexpr uint32_t kErrWord = 8;          // device error word
+constexpr uint32_t kStatsWords = 16;      // three u64 counters
+constexpr uint32_t kClassBounds = 32;     // [begin, count] per class
+constexpr uint32_t kHeavyBounds = 40;     // [0, heavy count]
 
 // Everything one counting pass needs, allocated once; enqueue may be
 // repeated and captured in a CUDA graph.
@@ -82,9 +95,10 @@ struct CountPlan {
   bool edge = false;
   uint32_t n_units = 0, max_size = 0;
   uint32_t *size = nullptr, *hist = nullptr, *rev = nullptr, *queue = nullptr, *scratch = nullptr;
+  uint32_t* heavy = nullptr;
   unsigned long long* d_out = nullptr;
-  PreparedLaunch launches[kNumClasses];
-  bool active[kNumClasses] = {false, false, false, false};
+  PreparedLaunch launches[kNumClasses + 1];
+  bool active[kNumClasses + 1] = {false, false, false, false, false};
 };
 
 kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long* d_out, uint32_t depth_boost,
@@ -94,5 +108,7 @@ void count_release(CountPlan* pl);
 // Reads the device error word (and the three stats counters when stats3 != null).
 uint32_t count_error(const CountPlan& pl, cudaStream_t s, unsigned long long* stats3);
 uint64_t count_units(const CountPlan& pl, cudaStream_t s);
+// Units the last enqueue handed to the heavy pass.
+uint32_t count_heavy(const CountPlan& pl, cudaStream_t s);
 
 }  // namespace kc

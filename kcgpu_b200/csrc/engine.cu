@@ -102,21 +102,24 @@ kc_status build_from_device(kc_graph* g, const uint32_t* d_src, const uint32_t* 
 }  // namespace
 
 kc_params autotune(uint32_t n, uint64_t m, uint32_t max_out, uint32_t k, uint32_t max_core) {
-  // Per-graph choice from shape features. Pivoting wins when the graph holds
-  // large cliques (its cost follows the clique tree, not the clique count);
-  // orientation listing wins on sparse graphs with few cliques. Word-width of
-  // the largest unit picks the partition size; edge units spread the work of
-  // graphs with few vertices but wide out-neighbourhoods.
+  // Per-graph choice from shape features.
+  //  * mode: pivoting wins when the graph holds large cliques (its cost follows
+  //    the clique tree, not the clique count); orientation listing wins on
+  //    sparse neighbourhoods. Graphs whose peel shows a dense core pivot
+  //    outright; the others run KC_MODE_AUTO, which lists small units and moves
+  //    any unit that outgrows its budget (a hidden clique) to the pivot.
+  //  * part: 0 lets each size class size its partitions to its word width.
+  //  * unit: edge units spread the work of graphs with few vertices but wide
+  //    out-neighbourhoods over more groups.
+  //  * encoding: sorted lists only for very wide, very sparse neighbourhoods.
   kc_params p;
   std::memset(&p, 0, sizeof(p));
   p.k = k;
   const double dens = n > 1 ? (2.0 * (double)m) / ((double)n * (n - 1)) : 0.0;
-  const bool dense_core = max_core >= 16 || (max_core + 1 >= k && k >= 7);
-  p.mode = (dense_core || k >= 9) ? KC_MODE_PIVOT : KC_MODE_ORIENT;
+  const bool dense_core = max_core >= 24 || (max_core + 1 >= k && k >= 7 && max_core >= 12);
+  p.mode = dense_core ? KC_MODE_PIVOT : KC_MODE_AUTO;
   p.unit = (n < 256 && max_out > 64) ? KC_UNIT_EDGE : KC_UNIT_NODE;
-  const uint32_t W = (max_out + 31) / 32;
-  if (p.mode == KC_MODE_ORIENT) p.part = W <= 1 ? 1 : (W <= 2 ? 2 : (W <= 4 ? 4 : (W <= 8 ? 8 : 16)));
-  else p.part = W <= 2 ? 4 : (W <= 4 ? 8 : (W <= 8 ? 16 : 32));
+  p.part = 0;
   p.encoding = (max_out > 4096 && dens < 0.001) ? KC_ENC_LIST : KC_ENC_BITMAP;
   return p;
 }
@@ -386,7 +389,7 @@ kc_status kc_parse_spec(const char* spec, kc_params* io) {
 kc_status kc_count(kc_graph* g, const kc_params* p, kc_u128* out, kc_count_stats* stats) {
   if (!g || !p || !out) return fail(KC_ERR_INVALID_ARG, "NULL argument");
   if (p->k < 1) return fail(KC_ERR_INVALID_ARG, "k must be >= 1");
-  if (p->mode > KC_MODE_PIVOT || p->unit > KC_UNIT_EDGE || p->encoding > KC_ENC_LIST)
+  if (p->mode > KC_MODE_AUTO || p->unit > KC_UNIT_EDGE || p->encoding > KC_ENC_LIST)
     return fail(KC_ERR_INVALID_ARG, "unknown mode, unit or encoding");
   if (p->part != 0 && (p->part > 32 || (p->part & (p->part - 1))))
     return fail(KC_ERR_INVALID_ARG, "partition size %u is not one of 1,2,4,8,16,32", p->part);

@@ -14,7 +14,7 @@ from tests import graphs as G
 
 pytestmark = pytest.mark.gpu
 
-VARIANTS = [(mode, unit, enc) for mode in ("orient", "pivot") for unit in ("node", "edge")
+VARIANTS = [(mode, unit, enc) for mode in ("orient", "pivot", "auto") for unit in ("node", "edge")
             for enc in ("bitmap", "list")]
 
 
@@ -148,6 +148,41 @@ def test_edgeless_union_multipartite(ctx):
                 want = G.multipartite_kcliques(sizes, k)
                 for mode, unit, enc in VARIANTS:
                     assert g.count(k, mode=mode, unit=unit, encoding=enc) == want, (sizes, k, mode, unit, enc)
+
+
+def test_heavy_units_handed_on(ctx):
+    # planted cliques of 28-32 vertices: the lowest clique vertex's unit needs
+    # far more traversal nodes than a warp unit's budget, so it is counted
+    # again by the CTA-wide heavy pass; the count must not change.
+    el = kc.gen_er(400, 0.04, 31)
+    el.plant_cliques(2, 28, 32, 8)
+    s, d, n = el.arrays()
+    og = OracleGraph(s, d, n)
+    og.orient("degree")
+    with kc.Graph.from_edges(ctx, s, d, n) as g:
+        g.orient("degree")
+        for k in (5, 7, 9):
+            want = og.count(k, "pivot")
+            for mode in ("orient", "pivot", "auto"):
+                for unit in ("node", "edge"):
+                    for part in (0, 4, 32):
+                        got = g.count(k, mode=mode, unit=unit, part=part)
+                        assert got == want, (k, mode, unit, part)
+
+
+def test_batched_matches_single_graph_counts(ctx):
+    e = kc.gen_batch(60, 77)
+    s, d, _ = e.arrays()
+    off, nn, kk, fam = e.batch_meta()
+    for orientation in ("degree", "degen"):
+        counts, choice, st = kc.batch_count(ctx, s, d, off, nn, kk, orientation=orientation, return_choice=True,
+                                            return_stats=True)
+        assert st["n_graphs"] == 60 and st["tree_nodes"] > 0
+        for g in range(60):
+            a, b = int(off[g]), int(off[g + 1])
+            og = OracleGraph(s[a:b], d[a:b], int(nn[g]))
+            og.orient(orientation)
+            assert counts[g] == og.count(int(kk[g]), "pivot"), (orientation, g, choice[g])
 
 
 def test_relabel_invariance(ctx):
