@@ -145,15 +145,19 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool 
   kc_status st = build_csr(&U, ds, dd, E, (uint32_t)N);
   cudaFreeAsync(ds, s);
   cudaFreeAsync(dd, s);
-  if (st == KC_OK) st = orient_graph(&U, orientation);
+  // graph of every original vertex: gives each graph a contiguous rank range
   if (st == KC_OK) {
     KC_CUDA(cudaMallocAsync(&vg, sizeof(uint32_t) * std::max<uint64_t>(1, N), s));
-    st = dev_alloc(&U, (void**)&U.vgraph, sizeof(uint32_t) * std::max<uint64_t>(1, N));
+    k_vertex_graph<<<std::min<uint32_t>(G, 65535), 256, 0, s>>>(dvoff, G, vg);
+    U.vgraph_orig = vg;
+    U.n_graphs = G;
+    st = orient_graph(&U, orientation);
+    U.vgraph_orig = nullptr;
   }
+  if (st == KC_OK) st = dev_alloc(&U, (void**)&U.vgraph, sizeof(uint32_t) * std::max<uint64_t>(1, N));
   std::vector<uint32_t> fmax(G, 0), fcore(G, 0);
   std::vector<unsigned long long> fm(G, 0);
   if (st == KC_OK) {
-    k_vertex_graph<<<std::min<uint32_t>(G, 65535), 256, 0, s>>>(dvoff, G, vg);
     k_rank_graph<<<grid_for(N, ctx->sms), 256, 0, s>>>(vg, U.rank, (uint32_t)N, U.vgraph);
     uint32_t *dfmax = nullptr, *dfcore = nullptr;
     unsigned long long* dfm = nullptr;

@@ -74,6 +74,10 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
   uint32_t* B = p.bitmap_global ? gb : sb + p.off_B;
   uint32_t* R0 = sb + p.off_R0;
   uint32_t* frames = (p.frames_global ? gb + p.goff_fr : sb + p.off_fr) + (size_t)part * p.depth * p.fw;
+  // open-addressing hash of S: vertex -> local index (linear probing, load <= 1/2)
+  const uint32_t hT = p.hash_T;
+  uint32_t* hkey = sb + p.off_H;
+  uint32_t* hval = hkey + hT;
 
   // class bounds come from device memory: clamp them so no unit index can leave the queue
   const uint32_t ubeg = min(p.bounds[2 * p.cls], p.n_units_max);
@@ -196,6 +200,17 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
 
     // ---- induced subgraph on S as a bitmap (row j, bit i: S[i] in N+(S[j]))
     for (uint32_t i = gt; i < d * W; i += G) B[i] = 0u;
+    const uint32_t hshift = hT ? 33u - (uint32_t)__ffs(hT) : 0u;  // 32 - log2(hT)
+    if (hT) {
+      for (uint32_t i = gt; i < hT; i += G) hkey[i] = 0xffffffffu;
+      gsync();
+      for (uint32_t i = gt; i < d; i += G) {
+        const uint32_t x = S[i];
+        uint32_t h = (x * 0x9e3779b1u) >> hshift;
+        while (atomicCAS(&hkey[h], 0xffffffffu, x) != 0xffffffffu) h = (h + 1u) & (hT - 1u);
+        hval[h] = i;
+      }
+    }
     gsync();
     {
       const uint32_t last = S[d - 1];
@@ -209,12 +224,21 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
           const bool inr = x <= last;
           if (!__any_sync(0xffffffffu, inr)) break;
           if (inr) {
-            uint32_t lo = j + 1, hi = d;
-            while (lo < hi) {
-              const uint32_t mid = (lo + hi) >> 1;
-              if (S[mid] < x) lo = mid + 1; else hi = mid;
+            uint32_t lo = 0xffffffffu;
+            if (hT) {
+              // the hash holds every vertex of S; x may be absent (a miss)
+              uint32_t h = (x * 0x9e3779b1u) >> hshift;
+              for (uint32_t key; (key = hkey[h]) != 0xffffffffu; h = (h + 1u) & (hT - 1u))
+                if (key == x) { lo = hval[h]; break; }
+            } else {
+              uint32_t a = j + 1, c = d;
+              while (a < c) {
+                const uint32_t mid = (a + c) >> 1;
+                if (S[mid] < x) a = mid + 1; else c = mid;
+              }
+              if (a < d && S[a] == x) lo = a;
             }
-            if (lo < d && S[lo] == x) {
+            if (lo != 0xffffffffu) {
               atomicOr(&B[j * W + (lo >> 5)], 1u << (lo & 31u));
               if (sym) atomicOr(&B[lo * W + (j >> 5)], 1u << (j & 31u));
             }
@@ -455,13 +479,20 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
   const size_t sB = (size_t)dcap * W;
   const size_t sFr = (size_t)nparts * depth * fw;
   const size_t limit_words = (size_t)ctx->max_smem_optin / 4;
+  // hash of S for the bitmap build: 2*hT words, hT the power of two >= 2 dcap
+  uint32_t hT = 0;
+  if (dcap <= 2048) {
+    hT = 64;
+    while (hT < 2 * dcap) hT <<= 1;
+  }
   bool bitmap_global = lp.force_global_bitmap;
   bool frames_global = false;
   auto group_words = [&]() {
-    return hdr + sS + sR0 + (bitmap_global ? 0 : al4(sB)) + (frames_global ? 0 : sFr);
+    return hdr + sS + sR0 + 2 * (size_t)hT + (bitmap_global ? 0 : al4(sB)) + (frames_global ? 0 : sFr);
   };
   if ((size_t)gpb * group_words() > limit_words) frames_global = true;
   if ((size_t)gpb * group_words() > limit_words) bitmap_global = true;
+  if ((size_t)gpb * group_words() > limit_words) hT = 0;
   if ((size_t)gpb * group_words() > limit_words)
     return fail(KC_ERR_INVALID_ARG, "unit size %u does not fit the shared-memory plan", dcap);
   p.dcap = dcap;
@@ -471,9 +502,11 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
   p.depth = depth;
   p.fw = fw;
   p.group_words = (uint32_t)group_words();
-  p.off_B = (uint32_t)(hdr + sS + sR0);
   p.off_R0 = (uint32_t)(hdr + sS);
-  p.off_fr = (uint32_t)(hdr + sS + sR0 + (bitmap_global ? 0 : al4(sB)));
+  p.off_H = (uint32_t)(hdr + sS + sR0);
+  p.hash_T = hT;
+  p.off_B = (uint32_t)(hdr + sS + sR0 + 2 * (size_t)hT);
+  p.off_fr = (uint32_t)(p.off_B + (bitmap_global ? 0 : al4(sB)));
   p.bitmap_global = bitmap_global;
   p.frames_global = frames_global;
   p.gbuf_words = (bitmap_global ? al4(sB) : 0) + (frames_global ? sFr : 0);

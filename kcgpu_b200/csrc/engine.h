@@ -42,7 +42,12 @@ struct kc_graph {
   uint32_t* prio = nullptr;  // reference-compatible peel priority (original ids)
   uint32_t* level = nullptr; // peel level = core number (original ids)
   uint32_t max_core = 0;
+  uint32_t peel_rounds = 0;  // sub-rounds that received a priority
   uint32_t* vgraph = nullptr; // batch: graph of every rank label (null for single graphs)
+  // batch: graph of every original vertex, set before kc_orient so each
+  // graph's vertices get one contiguous range of rank labels (null otherwise)
+  const uint32_t* vgraph_orig = nullptr;
+  uint32_t n_graphs = 0;
   uint64_t bytes = 0;
 };
 

@@ -43,15 +43,25 @@ uint32_t grid_for(uint64_t work, int sms, int per_sm = 16) {
   return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((work + 255) / 256, (uint64_t)sms * per_sm));
 }
 
-__global__ void k_degree_keys(const uint32_t* __restrict__ rp, uint32_t n, int vbits,
-                              unsigned long long* keys) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
-    keys[v] = ((unsigned long long)(rp[v + 1] - rp[v]) << vbits) | v;
+// Sort keys (graph, major, v): the graph field (batches only) is the most
+// significant so each graph's vertices get a contiguous range of ranks; it
+// never changes the order of two vertices of the same graph.
+__global__ void k_degree_keys(const uint32_t* __restrict__ rp, uint32_t n, int vbits, const uint32_t* __restrict__ vg,
+                              int gshift, unsigned long long* keys) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    unsigned long long k = ((unsigned long long)(rp[v + 1] - rp[v]) << vbits) | v;
+    if (vg) k |= (unsigned long long)vg[v] << gshift;
+    keys[v] = k;
+  }
 }
 
-__global__ void k_prio_keys(const uint32_t* __restrict__ prio, uint32_t n, int vbits, unsigned long long* keys) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
-    keys[v] = ((unsigned long long)prio[v] << vbits) | v;
+__global__ void k_prio_keys(const uint32_t* __restrict__ prio, uint32_t n, int vbits, uint32_t cap,
+                            const uint32_t* __restrict__ vg, int gshift, unsigned long long* keys) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    unsigned long long k = ((unsigned long long)min(prio[v], cap) << vbits) | v;
+    if (vg) k |= (unsigned long long)vg[v] << gshift;
+    keys[v] = k;
+  }
 }
 
 __global__ void k_rank_from_sorted(const unsigned long long* __restrict__ keys, uint32_t n,
@@ -331,6 +341,7 @@ kc_status peel_graph(kc_graph* g) {
   cudaFreeAsync(ba, s); cudaFreeAsync(bb, s); cudaFreeAsync(fa, s); cudaFreeAsync(fb, s); cudaFreeAsync(ctr, s);
   if (out[2]) return fail(KC_ERR_INTERNAL, "peel did not converge (device error %u)", out[2]);
   g->max_core = out[0];
+  g->peel_rounds = out[1];
   return KC_OK;
 }
 
@@ -360,15 +371,22 @@ kc_status orient_graph(kc_graph* g, uint32_t orientation) {
   KC_CUDA(cudaMallocAsync(&mx, sizeof(uint32_t), s));
   KC_CUDA(cudaMemsetAsync(mx, 0, sizeof(uint32_t), s));
   int major_bits;
+  const int graph_bits = g->vgraph_orig ? bits_for(g->n_graphs ? g->n_graphs - 1 : 0) : 0;
   if (orientation == KC_ORIENT_DEGREE) {
-    k_degree_keys<<<grid_for(n, ctx->sms), 256, 0, s>>>(g->rp, n, vbits, keys);
     major_bits = bits_for(g->max_deg);
+    k_degree_keys<<<grid_for(n, ctx->sms), 256, 0, s>>>(g->rp, n, vbits, g->vgraph_orig, vbits + major_bits, keys);
   } else {
-    k_prio_keys<<<grid_for(n, ctx->sms), 256, 0, s>>>(g->prio, n, vbits, keys);
-    major_bits = bits_for(std::min<uint64_t>(2 * g->m, 0xffffffffull));
+    // Peel priorities are sub-round indices below peel_rounds, except the
+    // final batch's 2m; capping that one at peel_rounds keeps every order and
+    // keeps the key narrow.
+    const uint32_t cap = (uint32_t)std::min<uint64_t>(std::min<uint64_t>(2 * g->m, 0xffffffffull), g->peel_rounds);
+    major_bits = bits_for(cap);
+    k_prio_keys<<<grid_for(n, ctx->sms), 256, 0, s>>>(g->prio, n, vbits, cap, g->vgraph_orig, vbits + major_bits,
+                                                    keys);
   }
   KC_CUDA(cudaGetLastError());
-  KC_CUDA(prim::radix_sort_u64(keys, tmp, n, vbits + major_bits, s));
+  if (vbits + major_bits + graph_bits > 64) return fail(KC_ERR_INTERNAL, "orientation key exceeds 64 bits");
+  KC_CUDA(prim::radix_sort_u64(keys, tmp, n, vbits + major_bits + graph_bits, s));
   k_rank_from_sorted<<<grid_for(n, ctx->sms), 256, 0, s>>>(keys, n, (vbits >= 64) ? ~0ull : ((1ull << vbits) - 1),
                                                           g->rank, g->inv);
   const uint32_t gw = grid_for((uint64_t)n * 32, ctx->sms, 32);

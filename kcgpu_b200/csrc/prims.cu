@@ -196,11 +196,12 @@ __global__ void __launch_bounds__(NT) k_radix_scatter(const unsigned long long* 
 
 // ---- segmented sort + dedup --------------------------------------------------
 
-enum RowClass { RC_TRIVIAL = 0, RC_WARP = 1, RC_B2K = 2, RC_B16K = 3, RC_B32K = 4, RC_HUGE = 5, RC_N = 6 };
+enum RowClass { RC_TRIVIAL = 0, RC_WARP = 1, RC_B2K = 2, RC_B16K = 3, RC_B32K = 4, RC_HUGE = 5, RC_W256 = 6, RC_N = 7 };
 
 __device__ __forceinline__ int row_class(uint32_t len) {
   if (len <= 1) return RC_TRIVIAL;
   if (len <= 32) return RC_WARP;
+  if (len <= 256) return RC_W256;
   if (len <= 2048) return RC_B2K;
   if (len <= 16384) return RC_B16K;
   if (len <= 32768) return RC_B32K;
@@ -255,6 +256,51 @@ __global__ void k_seg_warp(const uint32_t* __restrict__ off, uint32_t* data, uin
     uint32_t bal = __ballot_sync(0xffffffffu, keep);
     if (keep) data[b + __popc(bal & lanemask_lt())] = v;
     if (lane == 0) ucnt[r] = __popc(bal);
+  }
+}
+
+// Warp per row for rows of 33..256 entries: each warp sorts its own row in a
+// private 256-word shared buffer (bitonic, __syncwarp only), so a block works
+// on eight rows at once without block-wide barriers.
+__global__ void __launch_bounds__(256) k_seg_warp_smem(const uint32_t* __restrict__ off, uint32_t* data,
+                                                       uint32_t* ucnt, const uint32_t* __restrict__ list,
+                                                       const uint32_t* count, uint32_t n_rows) {
+  __shared__ uint32_t buf[8][256];
+  const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+  uint32_t* sm = buf[w];
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t cnt = min(*count, n_rows);
+  for (uint32_t li = gw; li < cnt; li += nw) {
+    const uint32_t r = list[li];
+    const uint32_t b = off[r], len = off[r + 1] - b;
+    if (len > 256) continue;  // never index past the buffer
+    uint32_t p2 = 32;
+    while (p2 < len) p2 <<= 1;
+    for (uint32_t i = lane; i < p2; i += 32) sm[i] = i < len ? data[b + i] : 0xffffffffu;
+    __syncwarp();
+    for (uint32_t k = 2; k <= p2; k <<= 1) {
+      for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+        for (uint32_t i = lane; i < p2; i += 32) {
+          const uint32_t ixj = i ^ j;
+          if (ixj > i) {
+            const uint32_t a = sm[i], c = sm[ixj];
+            if ((a > c) == ((i & k) == 0)) { sm[i] = c; sm[ixj] = a; }
+          }
+        }
+        __syncwarp();
+      }
+    }
+    uint32_t outpos = 0;
+    for (uint32_t c0 = 0; c0 < len; c0 += 32) {
+      const uint32_t i = c0 + lane;
+      const bool keep = i < len && (i == 0 || sm[i] != sm[i - 1]);
+      const uint32_t bal = __ballot_sync(0xffffffffu, keep);
+      if (keep) data[b + outpos + __popc(bal & lanemask_lt())] = sm[i];
+      outpos += __popc(bal);
+    }
+    if (lane == 0) ucnt[r] = outpos;
+    __syncwarp();
   }
 }
 
@@ -430,6 +476,9 @@ cudaError_t segmented_sort_unique(const uint32_t* off, uint32_t* data, uint32_t*
     uint32_t grid = (uint32_t)std::min<size_t>((n_rows + 255) / 256, (size_t)sms * 16);
     k_classify_rows<<<grid, 256, 0, s>>>(off, n_rows, ucount, lists, counts, huge_total);
   }
+  if (max_len > 32)
+    k_seg_warp_smem<<<sms * 8, 256, 0, s>>>(off, data, ucount, lists + (size_t)RC_W256 * n_rows, counts + RC_W256,
+                                            n_rows);
   k_seg_warp<<<sms * 8, 256, 0, s>>>(off, data, ucount, lists + (size_t)RC_WARP * n_rows, counts + RC_WARP,
                                      n_rows);
   if (max_len > 32)
