@@ -51,6 +51,97 @@ __device__ __forceinline__ uint32_t valid_mask(uint32_t d, uint32_t w) {  // bit
   return low_mask(d, w);
 }
 
+constexpr int kLaneStack = 16;  // lane-DFS levels: t - 2 <= 16, i.e. k <= 19 (node units)
+
+template <int NW>
+__device__ __forceinline__ void load_row(const uint32_t* B, uint32_t v, uint32_t (&r)[NW]) {
+  if constexpr (NW == 4) {
+    const uint4 q = *reinterpret_cast<const uint4*>(B + v * 4u);
+    r[0] = q.x; r[1] = q.y; r[2] = q.z; r[3] = q.w;
+  } else if constexpr (NW == 2) {
+    const uint2 q = *reinterpret_cast<const uint2*>(B + v * 2u);
+    r[0] = q.x; r[1] = q.y;
+  } else {
+    r[0] = B[v];
+  }
+}
+
+// Orientation traversal with one lane per second-level subtree: the candidate
+// set (NW words) lives in registers, rows come from shared memory with one
+// vector load, and a lane's stack holds only the sets of the levels above it.
+// Counts the t-cliques of the unit whose bitmap B has rows of stride NW.
+// Returns false when the unit ran over its budget (its count is then void).
+template <int NW>
+__device__ bool lane_dfs(const uint32_t* B, uint32_t d, uint32_t t, uint32_t* hdr, uint32_t budget,
+                         unsigned __int128& uacc, unsigned long long& st_nodes, unsigned long long& st_words) {
+  uint32_t stk[kLaneStack][NW];
+  unsigned long long cnt = 0;
+  uint32_t since = 0;
+  bool ok = true;
+  for (;;) {
+    if (budget && *(volatile uint32_t*)&hdr[5]) { ok = false; break; }
+    const uint32_t j = atomicAdd(&hdr[1], 1u);
+    if (j >= d) break;
+    uint32_t cur[NW];
+    load_row<NW>(B, j, cur);
+    uint32_t c = 0;
+#pragma unroll
+    for (int q = 0; q < NW; ++q) c += __popc(cur[q]);
+    st_nodes++;
+    st_words += NW;
+    if (t == 2u) { cnt += c; continue; }
+    if (c < t - 1u) continue;
+    int lv = 0;
+    for (;;) {
+      int w = -1;
+#pragma unroll
+      for (int q = NW - 1; q >= 0; --q)
+        if (cur[q]) w = q;
+      if (w < 0) {
+        if (lv == 0) break;
+        --lv;
+#pragma unroll
+        for (int q = 0; q < NW; ++q) cur[q] = stk[lv][q];
+        continue;
+      }
+      uint32_t word = 0;
+#pragma unroll
+      for (int q = 0; q < NW; ++q)
+        if (q == w) { word = cur[q]; cur[q] = word & (word - 1u); }
+      const uint32_t v = (uint32_t)w * 32u + (uint32_t)__ffs(word) - 1u;
+      uint32_t row[NW], child[NW];
+      load_row<NW>(B, v, row);
+      uint32_t n = 0;
+#pragma unroll
+      for (int q = 0; q < NW; ++q) {
+        child[q] = cur[q] & row[q];
+        n += __popc(child[q]);
+      }
+      st_nodes++;
+      st_words += NW;
+      const uint32_t rem = t - (uint32_t)(lv + 2);
+      if (rem == 1u) {
+        cnt += n;
+      } else if (n >= rem) {
+#pragma unroll
+        for (int q = 0; q < NW; ++q) {
+          stk[lv][q] = cur[q];
+          cur[q] = child[q];
+        }
+        ++lv;
+      }
+      if (budget && ++since >= 64u) {
+        since = 0;
+        if (atomicAdd(&hdr[4], 64u) + 64u > budget) hdr[5] = 1u;
+        if (*(volatile uint32_t*)&hdr[5]) { ok = false; break; }
+      }
+    }
+    if (!ok) break;
+  }
+  uacc += cnt;
+  return ok;
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
   extern __shared__ __align__(16) uint32_t smem[];
@@ -179,7 +270,9 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
       gsync();
       continue;
     }
-    const uint32_t W = (d + 31u) >> 5;
+    // row stride in words: the unit's own width, or the launch's fixed 1/2/4
+    // words when rows are read with one vector load by the lane traversal
+    const uint32_t W = p.lane_dfs ? p.W : (d + 31u) >> 5;
     const bool sym = MODE == 1;
 
     if (MODE == 0) {
@@ -249,7 +342,14 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
     }
     gsync();
 
-    if (MODE == 0) {
+    if (MODE == 0 && p.lane_dfs) {
+      // ---- orientation traversal, one lane per subtree
+      const uint32_t t = p.edge_units ? k - 2u : k - 1u;
+      const uint32_t bud = budgeted ? p.budget : 0u;
+      if (W == 1u) lane_dfs<1>(B, d, t, hdr, bud, uacc, st_nodes, st_words);
+      else if (W == 2u) lane_dfs<2>(B, d, t, hdr, bud, uacc, st_nodes, st_words);
+      else lane_dfs<4>(B, d, t, hdr, bud, uacc, st_nodes, st_words);
+    } else if (MODE == 0) {
       // ---- orientation traversal
       const uint32_t t = p.edge_units ? k - 2u : k - 1u;
       for (;;) {
@@ -457,18 +557,25 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
                          PreparedLaunch* out) {
   if (lp.encoding == KC_ENC_LIST) return prepare_launch_list(ctx, lp, p0, s, out);
   CountParams p = p0;
-  const uint32_t P = lp.part;
+  uint32_t P = lp.part;
   if (P == 0 || P > 32 || (P & (P - 1)) != 0)
     return fail(KC_ERR_INVALID_ARG, "partition size %u is not one of 1,2,4,8,16,32", P);
   const uint32_t G = lp.G, block = lp.block;
   const uint32_t dcap = std::max<uint32_t>(1, lp.dcap);
-  const uint32_t W = (dcap + 31) / 32;
+  uint32_t W = (dcap + 31) / 32;
+  const uint32_t t_max = lp.edge ? (lp.k_max >= 2 ? lp.k_max - 2 : 0) : lp.k_max - 1;
+  // Warp units in orientation mode run the lane-per-subtree traversal: one
+  // lane is one partition, rows have 1, 2 or 4 words, no frames in shared memory.
+  const bool lane = lp.mode == KC_MODE_ORIENT && G == 32 && dcap <= 128 && t_max <= (uint32_t)kLaneStack + 2;
+  if (lane) {
+    P = 1;
+    W = W <= 1 ? 1 : (W <= 2 ? 2 : 4);
+  }
   const uint32_t nparts = G / P;
   const uint32_t gpb = block / G;
   uint32_t depth, fw;
   if (lp.mode == KC_MODE_ORIENT) {
-    const uint32_t t = lp.edge ? (lp.k_max >= 2 ? lp.k_max - 2 : 0) : lp.k_max - 1;
-    depth = std::max<uint32_t>(1, t >= 2 ? t - 2 : 1);
+    depth = std::max<uint32_t>(1, t_max >= 2 ? t_max - 2 : 1);
     fw = W + 1;
   } else {
     depth = lp.depth_boost ? dcap + 2 : std::min<uint32_t>(dcap + 2, 64);
@@ -477,7 +584,7 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
   auto al4 = [](size_t x) { return (x + 3) & ~(size_t)3; };
   const size_t hdr = 16, sS = al4(dcap), sR0 = al4(W);
   const size_t sB = (size_t)dcap * W;
-  const size_t sFr = (size_t)nparts * depth * fw;
+  const size_t sFr = lane ? 0 : al4((size_t)nparts * depth * fw);
   const size_t limit_words = (size_t)ctx->max_smem_optin / 4;
   // hash of S for the bitmap build: 2*hT words, hT the power of two >= 2 dcap
   uint32_t hT = 0;
@@ -505,6 +612,7 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
   p.off_R0 = (uint32_t)(hdr + sS);
   p.off_H = (uint32_t)(hdr + sS + sR0);
   p.hash_T = hT;
+  p.lane_dfs = lane ? 1u : 0u;
   p.off_B = (uint32_t)(hdr + sS + sR0 + 2 * (size_t)hT);
   p.off_fr = (uint32_t)(p.off_B + (bitmap_global ? 0 : al4(sB)));
   p.bitmap_global = bitmap_global;

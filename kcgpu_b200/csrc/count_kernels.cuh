@@ -34,6 +34,7 @@ struct CountParams {
   uint32_t off_B, off_R0, off_fr;  // shared-memory offsets (words) inside a group
   uint32_t off_H;            // shared-memory offset of the hash of S (keys, then local indices)
   uint32_t hash_T;           // hash slots (power of two >= 2 dcap), 0 = binary search instead
+  uint32_t lane_dfs;         // orientation with one lane per subtree (rows of W = 1, 2 or 4 words)
   uint32_t bitmap_global, frames_global;
   uint32_t* gbuf;            // global scratch, gbuf_words per group
   size_t gbuf_words;
