@@ -193,8 +193,12 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
     lp.edge = pl->edge;
     lp.dcap = heavy_pass ? std::max<uint32_t>(1, std::min<uint32_t>(kWarpClassMax, pl->max_size))
                          : (uint32_t)std::max<int64_t>(1, std::min<int64_t>(kClasses[c].hi, pl->max_size));
-    lp.G = heavy_pass ? 256 : kClasses[c].G;
-    lp.block = heavy_pass ? 256 : kClasses[c].block;
+    // The heavy pass pivots clique-heavy units, whose clique tree is a short
+    // chain: warp groups suffice. Orientation mode keeps a CTA per unit there,
+    // since listing such a unit is long work that needs every partition.
+    const bool heavy_cta = heavy_pass && lp.mode == KC_MODE_ORIENT;
+    lp.G = heavy_pass ? (heavy_cta ? 256u : 32u) : kClasses[c].G;
+    lp.block = heavy_pass ? (heavy_cta ? 256u : 128u) : kClasses[c].block;
     lp.force_global_bitmap = (c == 0);
     lp.k_max = k_max;
     lp.part = req.part ? req.part : auto_part(lp.mode, (lp.dcap + 31) / 32);

@@ -305,7 +305,31 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
       }
     }
     gsync();
-    {
+    if (G == 32 && hT) {
+      // Warp unit: one lane per row, so the 32 rows' dependent loads
+      // (row pointer, then the out-list) are in flight together; rows of a
+      // warp unit are short, and a lane's consecutive reads hit L1.
+      const uint32_t last = S[d - 1];
+      for (uint32_t j = lane; j < d; j += 32) {
+        const uint32_t x0 = S[j];
+        const uint32_t b = p.rp[x0], e = p.rp[x0 + 1];
+        uint32_t i = b;
+        for (; i < e; ++i) {
+          const uint32_t x = __ldg(p.col + i);
+          if (x > last) break;
+          uint32_t h = (x * 0x9e3779b1u) >> hshift;
+          for (uint32_t key; (key = hkey[h]) != 0xffffffffu; h = (h + 1u) & (hT - 1u)) {
+            if (key == x) {
+              const uint32_t lo = hval[h];
+              atomicOr(&B[j * W + (lo >> 5)], 1u << (lo & 31u));
+              if (sym) atomicOr(&B[lo * W + (j >> 5)], 1u << (j & 31u));
+              break;
+            }
+          }
+        }
+        st_bytes += 4ull * (min(i + 1u, e) - b);
+      }
+    } else {
       const uint32_t last = S[d - 1];
       for (uint32_t j = wig; j < d; j += nwg) {
         const uint32_t x0 = S[j];
@@ -587,10 +611,11 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
   const size_t sFr = lane ? 0 : al4((size_t)nparts * depth * fw);
   const size_t limit_words = (size_t)ctx->max_smem_optin / 4;
   // hash of S for the bitmap build: 2*hT words, hT the power of two >= 2 dcap
+  // (>= 4 dcap for warp units, whose mostly-missing lookups then probe ~1.4 slots)
   uint32_t hT = 0;
   if (dcap <= 2048) {
     hT = 64;
-    while (hT < 2 * dcap) hT <<= 1;
+    while (hT < (G == 32 ? 4u : 2u) * dcap) hT <<= 1;
   }
   bool bitmap_global = lp.force_global_bitmap;
   bool frames_global = false;
