@@ -391,3 +391,76 @@ def batch_count(ctx: Context, src, dst, edge_off, n_nodes, ks, orientation="degr
     if return_stats:
         out.append({f: getattr(st, f) for f, _ in KcBatchStats._fields_})
     return out[0] if len(out) == 1 else tuple(out)
+
+
+# ---- serving -------------------------------------------------------------------
+
+class Server:
+    """Continuous-batching request server (kc_server): requests of different
+    graphs and k run on several device streams as slots and HBM free up."""
+
+    def __init__(self, ctx: Context, hbm_budget_bytes: int = 0, streams: int = 4, orientation="degen",
+                 autotune: bool = True, fixed: dict | None = None):
+        o = _lib.KcServerOpts()
+        o.hbm_budget_bytes = int(hbm_budget_bytes)
+        o.streams = int(streams)
+        o.max_inflight = int(streams)
+        o.orientation = ORIENTATIONS[orientation] if isinstance(orientation, str) else int(orientation)
+        o.autotune = 1 if autotune else 0
+        if fixed:
+            o.fixed.mode = MODES[fixed.get("mode", "pivot")]
+            o.fixed.unit = UNITS[fixed.get("unit", "node")]
+            o.fixed.part = int(fixed.get("part", 8))
+            o.fixed.encoding = ENCODINGS[fixed.get("encoding", "bitmap")]
+        h = C.c_void_p()
+        check(lib().kc_server_create(ctx.handle, C.byref(o), C.byref(h)))
+        self._h = h
+        self.ctx = ctx
+
+    def put_graph(self, src, dst, n_nodes: int = 0) -> int:
+        s, d = _as_u32(src), _as_u32(dst)
+        gid = C.c_uint64()
+        check(lib().kc_server_put_graph(self._h, _u32p(s), _u32p(d), s.size, n_nodes, C.byref(gid)))
+        return int(gid.value)
+
+    def drop_graph(self, graph_id: int) -> None:
+        check(lib().kc_server_drop_graph(self._h, graph_id))
+
+    def submit(self, graph_id: int, k: int) -> int:
+        t = C.c_uint64()
+        check(lib().kc_server_submit(self._h, graph_id, k, C.byref(t)))
+        return int(t.value)
+
+    def submit_edges(self, src, dst, n_nodes: int, k: int) -> int:
+        s, d = _as_u32(src), _as_u32(dst)
+        t = C.c_uint64()
+        check(lib().kc_server_submit_edges(self._h, _u32p(s), _u32p(d), s.size, n_nodes, k, C.byref(t)))
+        return int(t.value)
+
+    def cancel(self, ticket: int) -> None:
+        check(lib().kc_server_cancel(self._h, ticket))
+
+    def wait(self, ticket: int, wait_ms: int = -1) -> dict:
+        r = _lib.KcRequestResult()
+        check(lib().kc_server_wait(self._h, ticket, wait_ms, C.byref(r)))
+        return {"count": r.count.value(), "status": int(r.status), "k": int(r.k), "submit_ms": r.submit_ms,
+                "start_ms": r.start_ms, "done_ms": r.done_ms, "graph_id": int(r.graph_id),
+                "params": {"mode": int(r.params.mode), "unit": int(r.params.unit), "part": int(r.params.part),
+                           "encoding": int(r.params.encoding)}}
+
+    def close(self):
+        if self._h:
+            lib().kc_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -455,20 +455,48 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
       for (uint32_t w = gt; w < W; w += G) R0[w] = ~B[p0 * W + w] & valid_mask(d, w);
       gsync();
 
+      auto binom = [&](uint32_t nn, uint32_t r) -> unsigned __int128 {
+        if (r > nn) return 0;
+        const unsigned long long* e = p.binom + 2ull * ((size_t)nn * (p.binom_cols + 1u) + r);
+        return ((unsigned __int128)e[1] << 64) | e[0];
+      };
+      // A clique-tree node with `hold` held vertices, `drop` pivots and the
+      // candidate set F[0, W) contributes sum_j C(drop, j) * cliques(G[F], r - j)
+      // with r = k - hold. For r <= 2 that sum is closed (cliques of size 0,
+      // 1, 2 are 1, |F| and the edges of G[F]), so the subtree is not walked.
+      // Otherwise the node's pivot and branch set are stored and it is pushed.
       auto enter = [&](uint32_t* F, uint32_t hold, uint32_t drop) -> bool {
         uint32_t nc = 0;
         for (uint32_t w = pt.plane; w < W; w += pt.P) nc += __popc(F[w]);
         nc = __reduce_add_sync(pt.pmask, nc);
+        const uint32_t r = k - hold;  // callers keep hold <= k
         if (nc == 0u) {
-          if (hold <= k && hold + drop >= k) {
-            const unsigned long long* e = p.binom + 2ull * ((size_t)drop * (p.binom_cols + 1u) + (k - hold));
-            uacc += ((unsigned __int128)e[1] << 64) | e[0];
-          }
+          uacc += binom(drop, r);
           return false;
         }
         if (hold + drop + nc < k) return false;
+        if (r <= 1u) {
+          uacc += (r == 0u) ? (unsigned __int128)1u : (unsigned __int128)(nc + drop);
+          return false;
+        }
+        // score every candidate u by |F ∩ N(u)|: lanes own words of F when F
+        // is wide, otherwise they take candidates in turn
         uint32_t best = 0;
-        if (W <= 4u) {
+        unsigned long long esum = 0;
+        if (W >= pt.P) {
+          for (uint32_t w = pt.plane; w < W; w += pt.P) {
+            uint32_t x = F[w];
+            while (x) {
+              const uint32_t b = __ffs(x) - 1u;
+              x &= x - 1u;
+              const uint32_t u = w * 32u + b;
+              uint32_t c = 0;
+              for (uint32_t q = 0; q < W; ++q) c += __popc(F[q] & B[u * W + q]);
+              esum += c;
+              best = max(best, (c << 16) | (0xffffu - u));
+            }
+          }
+        } else {
           uint32_t idx = 0;
           for (uint32_t w = 0; w < W; ++w) {
             uint32_t x = F[w];
@@ -479,25 +507,17 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
                 const uint32_t u = w * 32u + b;
                 uint32_t c = 0;
                 for (uint32_t q = 0; q < W; ++q) c += __popc(F[q] & B[u * W + q]);
+                esum += c;
                 best = max(best, (c << 16) | (0xffffu - u));
               }
             }
           }
-          st_words += (unsigned long long)nc * W / pt.P;
-        } else {
-          for (uint32_t w = 0; w < W; ++w) {
-            uint32_t x = F[w];
-            while (x) {
-              const uint32_t b = __ffs(x) - 1u;
-              x &= x - 1u;
-              const uint32_t u = w * 32u + b;
-              uint32_t c = 0;
-              for (uint32_t q = pt.plane; q < W; q += pt.P) c += __popc(F[q] & B[u * W + q]);
-              c = __reduce_add_sync(pt.pmask, c);
-              best = max(best, (c << 16) | (0xffffu - u));
-            }
-          }
-          st_words += (unsigned long long)nc * W;
+        }
+        st_words += (unsigned long long)nc * W / pt.P;
+        for (uint32_t o = 1; o < pt.P; o <<= 1) esum += __shfl_xor_sync(pt.pmask, esum, o);
+        if (r == 2u) {  // edges of G[F] + drop * |F| + C(drop, 2)
+          uacc += (unsigned __int128)(esum / 2u) + (unsigned __int128)drop * nc + binom(drop, 2u);
+          return false;
         }
         best = __reduce_max_sync(pt.pmask, best);
         const uint32_t piv = 0xffffu - (best & 0xffffu);

@@ -354,25 +354,44 @@ __global__ void __launch_bounds__(256) k_count_list(CountParams p, size_t cap_ed
       const uint32_t* Lp0 = row(p0);
       const uint32_t lp0 = rowlen(p0);
 
+      auto binom = [&](uint32_t nn, uint32_t r) -> unsigned __int128 {
+        if (r > nn) return 0;
+        const unsigned long long* e = p.binom + 2ull * ((size_t)nn * (p.binom_cols + 1u) + r);
+        return ((unsigned __int128)e[1] << 64) | e[0];
+      };
+      // A node with `hold` held vertices, `drop` pivots and candidates F[0, nc)
+      // contributes sum_j C(drop, j) * cliques(G[F], r - j), r = k - hold; for
+      // r <= 2 the sum is closed (1, |F| and the edges of G[F]).
       auto enter = [&](uint32_t* F, uint32_t nc, uint32_t hold, uint32_t drop) -> bool {
+        const uint32_t r = k - hold;  // callers keep hold <= k
         if (nc == 0u) {
-          if (hold <= k && hold + drop >= k) {
-            const unsigned long long* e = p.binom + 2ull * ((size_t)drop * (p.binom_cols + 1u) + (k - hold));
-            acc += ((unsigned __int128)e[1] << 64) | e[0];
-          }
+          acc += binom(drop, r);
           return false;
         }
         if (hold + drop + nc < k) return false;
+        if (r <= 1u) {
+          acc += (r == 0u) ? (unsigned __int128)1u : (unsigned __int128)(nc + drop);
+          return false;
+        }
+        // lanes take candidates in turn and score each by |F ∩ N(u)|
         uint32_t best = 0;
-        for (uint32_t a = 0; a < nc; ++a) {
+        unsigned long long esum = 0;
+        for (uint32_t a = pt.plane; a < nc; a += pt.P) {
           const uint32_t u = F[a];
           const uint32_t* Lu = row(u);
           const uint32_t lu = rowlen(u);
           uint32_t c = 0;
-          for (uint32_t q = pt.plane; q < nc; q += pt.P) c += bsearch_u32(Lu, lu, F[q]) ? 1u : 0u;
-          c = __reduce_add_sync(pt.pmask, c);
+          for (uint32_t q = 0; q < nc; ++q) c += bsearch_u32(Lu, lu, F[q]) ? 1u : 0u;
+          esum += c;
           best = max(best, (c << 16) | (0xffffu - u));
         }
+        for (uint32_t o = 1; o < pt.P; o <<= 1) esum += __shfl_xor_sync(pt.pmask, esum, o);
+        if (r == 2u) {
+          acc += (unsigned __int128)(esum / 2u) + (unsigned __int128)drop * nc + binom(drop, 2u);
+          st_words += (unsigned long long)nc * nc;
+          return false;
+        }
+        best = __reduce_max_sync(pt.pmask, best);
         st_words += (unsigned long long)nc * nc;
         const uint32_t piv = 0xffffu - (best & 0xffffu);
         const uint32_t* Lq = row(piv);

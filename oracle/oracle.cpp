@@ -170,9 +170,20 @@ struct PivotCounter {
     return c;
   }
 
-  void sct(std::vector<uint64_t>& C, uint32_t hold, uint32_t drop) {
+  // scratch for depth l: candidate set, branch set, earlier branches, child (4 W words)
+  std::vector<uint64_t> scratch;
+
+  uint64_t* level(uint32_t l) {
+    const size_t need = (size_t)(l + 2) * 4 * W;
+    if (scratch.size() < need) scratch.resize(need * 2);
+    return scratch.data() + (size_t)l * 4 * W;
+  }
+
+  // C is the candidate set stored in level(l)[0, W).
+  void sct(uint32_t l, uint32_t hold, uint32_t drop) {
     if (hold > k) return;
-    uint32_t nc = popc(C.data(), W);
+    uint64_t* C = level(l);
+    uint32_t nc = popc(C, W);
     if (nc == 0) {
       if (hold + drop >= k) total += B.get(drop, k - hold);
       return;
@@ -191,27 +202,38 @@ struct PivotCounter {
         if (best == UINT32_MAX || c > bestc) { best = v; bestc = c; }
       }
     }
+    level(l + 1);  // grow the scratch before taking pointers into it
+    C = level(l);
+    uint64_t* branch = C + W;
+    uint64_t* earlier = C + 2 * W;
     const uint64_t* ap = adj.data() + (size_t)best * W;
-    std::vector<uint64_t> branch(W), earlier(W, 0), child(W);
-    for (uint32_t w = 0; w < W; ++w) branch[w] = C[w] & ~ap[w];
+    for (uint32_t w = 0; w < W; ++w) {
+      branch[w] = C[w] & ~ap[w];
+      earlier[w] = 0;
+    }
     for (uint32_t w = 0; w < W; ++w) {
       uint64_t x = branch[w];
       while (x) {
         uint32_t v = w * 64 + (uint32_t)__builtin_ctzll(x);
         x &= x - 1;
         const uint64_t* av = adj.data() + (size_t)v * W;
+        uint64_t* child = level(l + 1);
+        C = level(l);
+        earlier = C + 2 * W;
         for (uint32_t q = 0; q < W; ++q) child[q] = C[q] & av[q] & ~earlier[q];
-        if (v == best) sct(child, hold, drop + 1);
-        else sct(child, hold + 1, drop);
-        earlier[v / 64] |= 1ull << (v % 64);
+        if (v == best) sct(l + 1, hold, drop + 1);
+        else sct(l + 1, hold + 1, drop);
+        C = level(l);  // the scratch may have grown during the recursion
+        C[2 * W + v / 64] |= 1ull << (v % 64);
       }
     }
   }
 
   void run(uint32_t hold) {
-    std::vector<uint64_t> C(W, 0);
+    uint64_t* C = level(0);
+    for (uint32_t w = 0; w < W; ++w) C[w] = 0;
     for (uint32_t i = 0; i < d; ++i) C[i / 64] |= 1ull << (i % 64);
-    sct(C, hold, 0);
+    sct(0, hold, 0);
   }
 };
 

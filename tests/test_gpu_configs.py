@@ -1,0 +1,81 @@
+"""The single-graph configurations at full size.
+
+At full size the CPU oracle would take minutes, so these tests check
+size-independent properties: every algorithm (orientation listing, pivoting,
+node and edge units) gives the same exact count, and planted cliques bound the
+count from below. The same generators at a smaller scale are compared with the
+oracle exactly.
+"""
+import math
+
+import pytest
+
+import kcgpu_b200 as kc
+from oracle.oracle import OracleGraph
+
+pytestmark = pytest.mark.gpu
+
+
+def test_rmat_scale16_matches_oracle(ctx):
+    # the CPU Pivoter needs ~10 s here at k = 5 (minutes at k = 7), so k = 7 is
+    # checked as agreement between the engine's algorithms
+    s, d, n = kc.gen_rmat(16, 16, 0.57, 0.19, 0.19, seed=20).arrays()
+    og = OracleGraph(s, d, n)
+    og.orient("degen")
+    with kc.Graph.from_edges(ctx, s, d, n) as g:
+        g.orient("degen")
+        want = og.count(5, "pivot", "node")
+        assert g.count(5, mode="pivot", unit="edge", part=8, encoding="bitmap") == want
+        assert g.count(5, mode="auto", unit="node", part=0) == want
+        assert g.count(5, mode="orient", unit="node", part=0) == want
+        c7 = g.count(7, mode="pivot", unit="edge", part=8, encoding="bitmap")
+        assert g.count(7, mode="pivot", unit="node", part=0) == c7
+        assert g.count(7, mode="auto", unit="edge", part=0) == c7
+
+
+def test_rmat_scale20_edge_factor16(ctx):
+    # R-MAT scale 20, edge factor 16, (a,b,c,d) = (0.57,0.19,0.19,0.05), degeneracy
+    # orientation, pivoting on edge units with partition 8 and bitmaps; k = 5 and 7
+    s, d, n = kc.gen_rmat(20, 16, 0.57, 0.19, 0.19, seed=1).arrays()
+    with kc.Graph.from_edges(ctx, s, d, n) as g:
+        g.orient("degen")
+        info = g.info()
+        assert info["n"] == 1 << 20 and 10_000_000 < info["m"] < 16_000_000
+        for k in (5, 7):
+            ref = g.count(k, mode="pivot", unit="edge", part=8, encoding="bitmap")
+            assert ref > 0
+            assert g.count(k, mode="pivot", unit="node", part=8) == ref
+            assert g.count(k, mode="auto", unit="node", part=0) == ref
+
+
+def test_chung_lu_4m_planted_cliques(ctx):
+    # Chung-Lu, exponent 2.1, n = 4M, mean degree 20, degree cap 50k, plus 200
+    # planted cliques of 30-60 vertices; pivoting with k = 3..12, 128-bit counts
+    el = kc.gen_chung_lu(4_000_000, 2.1, 20.0, 50_000.0, 3)
+    el.plant_cliques(200, 30, 60, 11)
+    s, d, n = el.arrays()
+    with kc.Graph.from_edges(ctx, s, d, n) as g:
+        g.orient("degen")
+        core, mx = g.kcore()
+        assert mx >= 29  # every planted clique of s vertices is an (s-1)-core
+        for k in (3, 6, 9, 12):
+            a = g.count(k, mode="pivot", unit="node", part=0)
+            b = g.count(k, mode="pivot", unit="edge", part=0)
+            assert a == b
+            if k <= 6:
+                assert g.count(k, mode="auto", unit="node", part=0) == a
+
+
+def test_chung_lu_small_planted_matches_oracle(ctx):
+    el = kc.gen_chung_lu(100_000, 2.1, 20.0, 2_000.0, 5)
+    el.plant_cliques(10, 30, 40, 7)
+    s, d, n = el.arrays()
+    og = OracleGraph(s, d, n)
+    og.orient("degen")
+    with kc.Graph.from_edges(ctx, s, d, n) as g:
+        g.orient("degen")
+        for k in (3, 8, 12):
+            want = og.count(k, "pivot")
+            assert want >= 10 * math.comb(30, k)  # ten disjoint planted cliques of >= 30 vertices
+            assert g.count(k, mode="pivot", unit="node", part=0) == want
+            assert g.count(k, mode="pivot", unit="edge", part=8) == want
