@@ -94,6 +94,13 @@ typedef struct kc_count_stats {
   double   ms_traversal;   /* device time of the traversal kernels */
   uint32_t max_unit_size;  /* largest induced subgraph (vertices) */
   uint32_t kernels;        /* kernels launched by the call */
+  double   ms_launch[5];   /* device time of each size-class launch (units > 1024,
+                              (128,1024], (32,128], <= 32 vertices) and of the
+                              heavy pass; 0 where nothing was launched */
+  uint64_t heavy_units;    /* units handed on to the heavy pass */
+  uint32_t deep_retry;     /* 1 when a clique tree outgrew the fast stack and the
+                              count was rerun with the full depth */
+  uint32_t reserved;
 } kc_count_stats;
 
 typedef struct kc_graph_info {

@@ -188,7 +188,9 @@ class Graph:
         st = KcCountStats()
         check(lib().kc_count(self._h, C.byref(p), C.byref(out), C.byref(st)))
         if stats:
-            return CountResult(out.value(), {f: getattr(st, f) for f, _ in KcCountStats._fields_})
+            vals = {f: getattr(st, f) for f, _ in KcCountStats._fields_ if f != "reserved"}
+            vals["ms_launch"] = list(vals["ms_launch"])
+            return CountResult(out.value(), vals)
         return out.value()
 
     def kcore(self):

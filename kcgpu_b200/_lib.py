@@ -28,7 +28,8 @@ class KcParams(C.Structure):
 class KcCountStats(C.Structure):
     _fields_ = [("units", u64), ("tree_nodes", u64), ("word_ops", u64), ("gather_bytes", u64),
                 ("ms_total", C.c_double), ("ms_traversal", C.c_double), ("max_unit_size", u32),
-                ("kernels", u32)]
+                ("kernels", u32), ("ms_launch", C.c_double * 5), ("heavy_units", u64), ("deep_retry", u32),
+                ("reserved", u32)]
 
 
 class KcGraphInfo(C.Structure):

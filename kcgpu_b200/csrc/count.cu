@@ -108,7 +108,11 @@ __global__ void k_unit_scatter(const uint32_t* __restrict__ size, uint32_t n_uni
 
 uint32_t auto_part(uint32_t mode, uint32_t W) {
   if (mode == KC_MODE_ORIENT) return W <= 1 ? 1u : (W <= 2 ? 2u : (W <= 4 ? 4u : (W <= 8 ? 8u : (W <= 16 ? 16u : 32u))));
-  return W <= 2 ? 4u : (W <= 4 ? 8u : (W <= 8 ? 16u : 32u));
+  // pivoting: a whole warp per clique-tree node. Partitions of one warp walk
+  // different nodes and so run one after another; a full warp scores the
+  // node's candidates one per lane instead.
+  (void)W;
+  return 32u;
 }
 
 }  // namespace
@@ -145,6 +149,19 @@ void count_release(CountPlan* pl) {
   for (void* p : ps)
     if (p) cudaFreeAsync(p, s);
   pl->size = pl->hist = pl->rev = pl->queue = pl->scratch = pl->heavy = nullptr;
+  for (int c = 0; c < kNumClasses; ++c) {
+    if (pl->side[c]) cudaStreamDestroy(pl->side[c]);
+    if (pl->join[c]) cudaEventDestroy(pl->join[c]);
+    pl->side[c] = nullptr;
+    pl->join[c] = nullptr;
+  }
+  if (pl->fork) cudaEventDestroy(pl->fork);
+  pl->fork = nullptr;
+  for (int c = 0; c <= kNumClasses; ++c) {
+    if (pl->tbeg[c]) cudaEventDestroy(pl->tbeg[c]);
+    if (pl->tend[c]) cudaEventDestroy(pl->tend[c]);
+    pl->tbeg[c] = pl->tend[c] = nullptr;
+  }
 }
 
 // Allocates the queue and the class launches. No kernel runs; the plan can be
@@ -155,7 +172,14 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
   cudaStream_t s = ctx->stream;
   pl->g = g;
   pl->req = req;
-  pl->edge = req.unit == KC_UNIT_EDGE;
+  // Edge units are grouped by source when the sources' out-neighbourhoods
+  // fit a shared-memory bitmap: the unit u builds G[N+(u)] once and its
+  // edges (u, v) are the root branches, each with the subproblem
+  // N+(u) ∩ N+(v), the row of v. Orientation listing walks exactly those
+  // branches for a node unit, so there the grouped form is the node form.
+  const bool grouped = req.unit == KC_UNIT_EDGE && req.encoding == KC_ENC_BITMAP && g->max_out <= 1024;
+  pl->edge = req.unit == KC_UNIT_EDGE && !grouped;
+  pl->edge_roots = grouped;
   pl->d_out = d_out;
   const uint32_t k_max = std::max(req.k, req.k_max);
   if (pl->edge) KC_TRY(ensure_edge_rows(g));
@@ -193,15 +217,14 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
     lp.edge = pl->edge;
     lp.dcap = heavy_pass ? std::max<uint32_t>(1, std::min<uint32_t>(kWarpClassMax, pl->max_size))
                          : (uint32_t)std::max<int64_t>(1, std::min<int64_t>(kClasses[c].hi, pl->max_size));
-    // The heavy pass pivots clique-heavy units, whose clique tree is a short
-    // chain: warp groups suffice. Orientation mode keeps a CTA per unit there,
-    // since listing such a unit is long work that needs every partition.
-    const bool heavy_cta = heavy_pass && lp.mode == KC_MODE_ORIENT;
-    lp.G = heavy_pass ? (heavy_cta ? 256u : 32u) : kClasses[c].G;
-    lp.block = heavy_pass ? (heavy_cta ? 256u : 128u) : kClasses[c].block;
+    // The heavy pass takes the units that outran a warp's budget: a CTA per
+    // unit, its partitions sharing the unit's clique tree.
+    lp.G = heavy_pass ? 256u : kClasses[c].G;
+    lp.block = heavy_pass ? 256u : kClasses[c].block;
     lp.force_global_bitmap = (c == 0);
     lp.k_max = k_max;
     lp.part = req.part ? req.part : auto_part(lp.mode, (lp.dcap + 31) / 32);
+    lp.q = lp.mode == KC_MODE_ORIENT ? 0u : req.part;
     lp.depth_boost = depth_boost;
     CountParams p;
     std::memset(&p, 0, sizeof(p));
@@ -213,6 +236,7 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
     p.cls = heavy_pass ? 0u : (uint32_t)c;
     p.n_units_max = pl->n_units;
     p.edge_units = pl->edge ? 1 : 0;
+    p.edge_roots = pl->edge_roots ? 1 : 0;
     p.vgraph = g->vgraph;
     p.gk = req.d_graph_k;
     p.k0 = req.k;
@@ -231,7 +255,17 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
     }
     KC_TRY(prepare_launch(ctx, lp, p, s, &pl->launches[c]));
     pl->active[c] = true;
+    if (!heavy_pass) {
+      KC_CUDA(cudaStreamCreateWithFlags(&pl->side[c], cudaStreamNonBlocking));
+      KC_CUDA(cudaEventCreateWithFlags(&pl->join[c], cudaEventDisableTiming));
+    }
   }
+  KC_CUDA(cudaEventCreateWithFlags(&pl->fork, cudaEventDisableTiming));
+  if (pl->timed)
+    for (int c = 0; c <= kNumClasses; ++c) {
+      KC_CUDA(cudaEventCreate(&pl->tbeg[c]));
+      KC_CUDA(cudaEventCreate(&pl->tend[c]));
+    }
   return KC_OK;
 }
 
@@ -252,9 +286,22 @@ kc_status count_enqueue(const CountPlan& pl, cudaStream_t s) {
   k_class_bounds<<<1, 32, 0, s>>>(pl.rev, M, pl.scratch + kClassBounds);
   if (pl.n_units) k_unit_scatter<<<gq, 256, 0, s>>>(pl.size, pl.n_units, M, pl.rev, pl.queue);
   KC_CUDA(cudaGetLastError());
-  // class launches, then the heavy pass over the units they handed on
-  for (int c = 0; c <= kNumClasses; ++c)
-    if (pl.active[c]) KC_TRY(enqueue_launch(pl.launches[c], s));
+  // class launches side by side, then the heavy pass over the units they handed on
+  KC_CUDA(cudaEventRecord(pl.fork, s));
+  for (int c = 0; c < kNumClasses; ++c) {
+    if (!pl.active[c]) continue;
+    KC_CUDA(cudaStreamWaitEvent(pl.side[c], pl.fork, 0));
+    if (pl.timed) KC_CUDA(cudaEventRecord(pl.tbeg[c], pl.side[c]));
+    KC_TRY(enqueue_launch(pl.launches[c], pl.side[c]));
+    if (pl.timed) KC_CUDA(cudaEventRecord(pl.tend[c], pl.side[c]));
+    KC_CUDA(cudaEventRecord(pl.join[c], pl.side[c]));
+    KC_CUDA(cudaStreamWaitEvent(s, pl.join[c], 0));
+  }
+  if (pl.active[kNumClasses]) {
+    if (pl.timed) KC_CUDA(cudaEventRecord(pl.tbeg[kNumClasses], s));
+    KC_TRY(enqueue_launch(pl.launches[kNumClasses], s));
+    if (pl.timed) KC_CUDA(cudaEventRecord(pl.tend[kNumClasses], s));
+  }
   return KC_OK;
 }
 
@@ -290,13 +337,17 @@ kc_status count_graph(kc_graph* g, const CountRequest& req, unsigned long long* 
   cudaEventCreate(&ev1);
   kc_status st = KC_OK;
   uint32_t kernels = 0;
-  uint64_t units = 0;
+  uint64_t units = 0, heavy = 0;
   unsigned long long sv[3] = {0, 0, 0};
+  double ms_launch[kNumClasses + 1] = {};
+  uint32_t deep = 0;
   for (uint32_t boost = 0; boost < 2; ++boost) {
     CountPlan pl;
+    pl.timed = stats != nullptr;
+    deep = boost;
     st = count_prepare(g, req, d_out, boost, &pl);
     if (st == KC_OK) {
-      cudaEventRecord(ev0, s);
+      if (boost == 0) cudaEventRecord(ev0, s);
       st = count_enqueue(pl, s);
       cudaEventRecord(ev1, s);
     }
@@ -304,6 +355,14 @@ kc_status count_graph(kc_graph* g, const CountRequest& req, unsigned long long* 
     if (st == KC_OK) {
       err = count_error(pl, s, sv);
       units = count_units(pl, s);
+      heavy = count_heavy(pl, s);
+      for (int c = 0; c <= kNumClasses; ++c) {
+        float t = 0;
+        if (pl.timed && pl.active[c] && cudaEventElapsedTime(&t, pl.tbeg[c], pl.tend[c]) == cudaSuccess)
+          ms_launch[c] = t;
+        else
+          ms_launch[c] = 0;
+      }
       kernels = 5;
       for (int c = 0; c <= kNumClasses; ++c) kernels += pl.active[c] ? 1 : 0;
     }
@@ -328,6 +387,10 @@ kc_status count_graph(kc_graph* g, const CountRequest& req, unsigned long long* 
     stats->ms_traversal = ms;
     stats->max_unit_size = g->max_out;
     stats->kernels = kernels;
+    for (int c = 0; c <= kNumClasses; ++c) stats->ms_launch[c] = ms_launch[c];
+    stats->heavy_units = heavy;
+    stats->deep_retry = deep;
+    stats->reserved = 0;
   }
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);

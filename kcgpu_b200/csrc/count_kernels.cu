@@ -164,7 +164,8 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
   uint32_t* S = sb + 16;
   uint32_t* B = p.bitmap_global ? gb : sb + p.off_B;
   uint32_t* R0 = sb + p.off_R0;
-  uint32_t* frames = (p.frames_global ? gb + p.goff_fr : sb + p.off_fr) + (size_t)part * p.depth * p.fw;
+  uint32_t* frames = (p.frames_global ? gb + p.goff_fr : sb + p.off_fr) + (size_t)part * p.pstride;
+  uint32_t* cand = frames + (size_t)p.depth * p.fw;  // pivoting: the candidates of the node being entered
   // open-addressing hash of S: vertex -> local index (linear probing, load <= 1/2)
   const uint32_t hT = p.hash_T;
   uint32_t* hkey = sb + p.off_H;
@@ -274,6 +275,9 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
     // words when rows are read with one vector load by the lane traversal
     const uint32_t W = p.lane_dfs ? p.W : (d + 31u) >> 5;
     const bool sym = MODE == 1;
+    // pivoting reads 32 rows at once (one candidate per lane): an odd row
+    // stride puts them in distinct shared-memory banks
+    const uint32_t Ws = sym ? (W | 1u) : W;
 
     if (MODE == 0) {
       const uint32_t t = p.edge_units ? k - 2u : k - 1u;
@@ -283,16 +287,17 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
         continue;
       }
     } else {
+      // k - hold0 <= 1: the unit's count is 1 (the unit is the clique) or d
       const uint32_t hold0 = p.edge_units ? 2u : 1u;
-      if (d == 0u || hold0 + d < k) {
-        if (part == 0 && d == 0u && k == hold0) acc += 1u;
+      if (d == 0u || hold0 + d < k || k <= hold0 + 1u) {
+        if (part == 0 && k >= hold0 && hold0 + d >= k) acc += (k == hold0) ? 1u : d;
         gsync();
         continue;
       }
     }
 
     // ---- induced subgraph on S as a bitmap (row j, bit i: S[i] in N+(S[j]))
-    for (uint32_t i = gt; i < d * W; i += G) B[i] = 0u;
+    for (uint32_t i = gt; i < d * Ws; i += G) B[i] = 0u;
     const uint32_t hshift = hT ? 33u - (uint32_t)__ffs(hT) : 0u;  // 32 - log2(hT)
     if (hT) {
       for (uint32_t i = gt; i < hT; i += G) hkey[i] = 0xffffffffu;
@@ -321,8 +326,8 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
           for (uint32_t key; (key = hkey[h]) != 0xffffffffu; h = (h + 1u) & (hT - 1u)) {
             if (key == x) {
               const uint32_t lo = hval[h];
-              atomicOr(&B[j * W + (lo >> 5)], 1u << (lo & 31u));
-              if (sym) atomicOr(&B[lo * W + (j >> 5)], 1u << (j & 31u));
+              atomicOr(&B[j * Ws + (lo >> 5)], 1u << (lo & 31u));
+              if (sym) atomicOr(&B[lo * Ws + (j >> 5)], 1u << (j & 31u));
               break;
             }
           }
@@ -356,8 +361,8 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
               if (a < d && S[a] == x) lo = a;
             }
             if (lo != 0xffffffffu) {
-              atomicOr(&B[j * W + (lo >> 5)], 1u << (lo & 31u));
-              if (sym) atomicOr(&B[lo * W + (j >> 5)], 1u << (j & 31u));
+              atomicOr(&B[j * Ws + (lo >> 5)], 1u << (lo & 31u));
+              if (sym) atomicOr(&B[lo * Ws + (j >> 5)], 1u << (j & 31u));
             }
           }
         }
@@ -365,6 +370,19 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
       }
     }
     gsync();
+
+    if (MODE == 1 && k == (p.edge_units ? 4u : 3u)) {
+      // k - hold0 = 2: the unit's count is the number of edges of G[S]
+      if (part == 0) {
+        unsigned long long e2 = 0;  // twice the edges: the bitmap is symmetric
+        for (uint32_t j = pt.plane; j < d; j += pt.P)
+          for (uint32_t w = 0; w < W; ++w) e2 += __popc(B[j * Ws + w]);
+        for (uint32_t o = 1; o < pt.P; o <<= 1) e2 += __shfl_xor_sync(pt.pmask, e2, o);
+        acc += e2 / 2u;
+      }
+      gsync();
+      continue;
+    }
 
     if (MODE == 0 && p.lane_dfs) {
       // ---- orientation traversal, one lane per subtree
@@ -435,25 +453,35 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
       }
     } else {
       // ---- pivot traversal (succinct clique tree)
+      // Root: a pivot p0 of G[S] and its branches R0 = S \ N(p0). With edge
+      // roots the root has no pivot: every v in S is a branch, the edge
+      // (u, S[v]) whose subproblem is N+(u) ∩ N+(S[v]), the bits above v of
+      // row v.
       const uint32_t hold0 = p.edge_units ? 2u : 1u;
-      uint32_t key = 0;
-      for (uint32_t v = gt; v < d; v += G) {
-        uint32_t c = 0;
-        for (uint32_t w = 0; w < W; ++w) c += __popc(B[v * W + w]);
-        key = max(key, (c << 16) | (0xffffu - v));
-      }
-      key = __reduce_max_sync(0xffffffffu, key);
-      if (lane == 0) hdr[8 + wig] = key;
-      gsync();
-      if (gt == 0) {
-        uint32_t m = 0;
-        for (uint32_t q = 0; q < nwg; ++q) m = max(m, hdr[8 + q]);
-        hdr[3] = 0xffffu - (m & 0xffffu);
+      if (p.edge_roots) {
+        if (gt == 0) hdr[3] = 0xffffffffu;
+        for (uint32_t w = gt; w < W; w += G) R0[w] = valid_mask(d, w);
+      } else {
+        uint32_t key = 0;
+        for (uint32_t v = gt; v < d; v += G) {
+          uint32_t c = 0;
+          for (uint32_t w = 0; w < W; ++w) c += __popc(B[v * Ws + w]);
+          key = max(key, (c << 16) | (0xffffu - v));
+        }
+        key = __reduce_max_sync(0xffffffffu, key);
+        if (lane == 0) hdr[8 + wig] = key;
+        gsync();
+        if (gt == 0) {
+          uint32_t m = 0;
+          for (uint32_t q = 0; q < nwg; ++q) m = max(m, hdr[8 + q]);
+          hdr[3] = 0xffffu - (m & 0xffffu);
+        }
+        gsync();
+        const uint32_t q0 = hdr[3];
+        for (uint32_t w = gt; w < W; w += G) R0[w] = ~B[q0 * Ws + w] & valid_mask(d, w);
       }
       gsync();
       const uint32_t p0 = hdr[3];
-      for (uint32_t w = gt; w < W; w += G) R0[w] = ~B[p0 * W + w] & valid_mask(d, w);
-      gsync();
 
       auto binom = [&](uint32_t nn, uint32_t r) -> unsigned __int128 {
         if (r > nn) return 0;
@@ -465,63 +493,79 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
       // with r = k - hold. For r <= 2 that sum is closed (cliques of size 0,
       // 1, 2 are 1, |F| and the edges of G[F]), so the subtree is not walked.
       // Otherwise the node's pivot and branch set are stored and it is pushed.
-      auto enter = [&](uint32_t* F, uint32_t hold, uint32_t drop) -> bool {
+      // Frame: F [0, W), branches R [W, 2W), then hold, drop, pivot, cursor.
+      // The pivot's branch goes last and reuses its parent's slot (nothing of
+      // the parent is needed after it), so only non-pivot branches, which
+      // each hold one more vertex, deepen the stack: at most k - hold0 + 1
+      // levels, whatever the length of the drop chains.
+      auto enter = [&](uint32_t* F, uint32_t hold, uint32_t drop, bool own) -> bool {
         uint32_t nc = 0;
         for (uint32_t w = pt.plane; w < W; w += pt.P) nc += __popc(F[w]);
         nc = __reduce_add_sync(pt.pmask, nc);
         const uint32_t r = k - hold;  // callers keep hold <= k
         if (nc == 0u) {
-          uacc += binom(drop, r);
+          if (own) uacc += binom(drop, r);
           return false;
         }
         if (hold + drop + nc < k) return false;
         if (r <= 1u) {
-          uacc += (r == 0u) ? (unsigned __int128)1u : (unsigned __int128)(nc + drop);
+          if (own) uacc += (r == 0u) ? (unsigned __int128)1u : (unsigned __int128)(nc + drop);
           return false;
         }
-        // score every candidate u by |F ∩ N(u)|: lanes own words of F when F
-        // is wide, otherwise they take candidates in turn
+        // score every candidate u by |F ∩ N(u)|: the candidates are listed
+        // in order first (one pass over the words, a bit per lane), then the
+        // lanes take them in turn, so each lane scores ceil(nc / P) of them
         uint32_t best = 0;
         unsigned long long esum = 0;
-        if (W >= pt.P) {
-          for (uint32_t w = pt.plane; w < W; w += pt.P) {
-            uint32_t x = F[w];
-            while (x) {
-              const uint32_t b = __ffs(x) - 1u;
-              x &= x - 1u;
-              const uint32_t u = w * 32u + b;
-              uint32_t c = 0;
-              for (uint32_t q = 0; q < W; ++q) c += __popc(F[q] & B[u * W + q]);
-              esum += c;
-              best = max(best, (c << 16) | (0xffffu - u));
-            }
-          }
-        } else {
-          uint32_t idx = 0;
-          for (uint32_t w = 0; w < W; ++w) {
-            uint32_t x = F[w];
-            while (x) {
-              const uint32_t b = __ffs(x) - 1u;
-              x &= x - 1u;
-              if ((idx++ % pt.P) == pt.plane) {
-                const uint32_t u = w * 32u + b;
-                uint32_t c = 0;
-                for (uint32_t q = 0; q < W; ++q) c += __popc(F[q] & B[u * W + q]);
-                esum += c;
-                best = max(best, (c << 16) | (0xffffu - u));
-              }
-            }
+        {
+          uint32_t base = 0;
+          for (uint32_t q = 0; q < W; ++q) {
+            const uint32_t x = F[q];
+            if (x == 0u) continue;
+            for (uint32_t b = pt.plane; b < 32u; b += pt.P)
+              if ((x >> b) & 1u) cand[base + __popc(x & ((1u << b) - 1u))] = q * 32u + b;
+            base += __popc(x);
           }
         }
-        st_words += (unsigned long long)nc * W / pt.P;
+        __syncwarp(pt.pmask);
+        // Q lanes score one candidate, each over every Q-th word: the
+        // launch's partition size, or (0) as many lanes as leave none idle
+        uint32_t Q = p.Q;
+        if (Q == 0u) {
+          Q = 1u;
+          while ((Q << 1) * nc <= pt.P && Q < W) Q <<= 1;
+        }
+        const uint32_t qs = (uint32_t)__ffs(Q) - 1u;  // Q is a power of two
+        const uint32_t ng = pt.P >> qs, gq = pt.plane >> qs, lq = pt.plane & (Q - 1u);
+        for (uint32_t i0 = 0; i0 < nc; i0 += ng) {
+          const uint32_t i = i0 + gq;
+          uint32_t c = 0, u = 0;
+          if (i < nc) {
+            u = cand[i];
+            const uint32_t* Bu = B + u * Ws;
+            for (uint32_t q = lq; q < W; q += Q) c += __popc(F[q] & Bu[q]);
+          }
+          for (uint32_t o = 1; o < Q; o <<= 1) c += __shfl_xor_sync(pt.pmask, c, o);
+          if (i < nc && lq == 0u) {
+            esum += c;
+            best = max(best, (c << 16) | (0xffffu - u));
+          }
+        }
+        if (own) st_words += (unsigned long long)nc * W / pt.P;
         for (uint32_t o = 1; o < pt.P; o <<= 1) esum += __shfl_xor_sync(pt.pmask, esum, o);
         if (r == 2u) {  // edges of G[F] + drop * |F| + C(drop, 2)
-          uacc += (unsigned __int128)(esum / 2u) + (unsigned __int128)drop * nc + binom(drop, 2u);
+          if (own) uacc += (unsigned __int128)(esum / 2u) + (unsigned __int128)drop * nc + binom(drop, 2u);
           return false;
         }
         best = __reduce_max_sync(pt.pmask, best);
         const uint32_t piv = 0xffffu - (best & 0xffffu);
-        for (uint32_t w = pt.plane; w < W; w += pt.P) F[W + w] = F[w] & ~B[piv * W + w];
+        // branch set: candidates outside N(piv), less the pivot itself, whose
+        // branch is taken last in this frame's own slot
+        for (uint32_t w = pt.plane; w < W; w += pt.P) {
+          uint32_t rw = F[w] & ~B[piv * Ws + w];
+          if (w == (piv >> 5)) rw &= ~(1u << (piv & 31u));
+          F[W + w] = rw;
+        }
         __syncwarp(pt.pmask);
         if (pt.plane == 0) {
           F[2 * W] = hold;
@@ -533,48 +577,82 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
         return true;
       };
 
-      for (;;) {
+      // Work split inside the unit: the clique tree (root at depth 0) is cut
+      // at depth L and the nodes at depth L go out by ticket (hdr[1]) to the
+      // group's partitions. Every partition walks the levels above the cut
+      // itself, re-deriving the same pivots, so no frame crosses partitions;
+      // partition 0 alone adds what the nodes above the cut contribute.
+      // L grows when the root has few branches (dense units, whose pivot
+      // neighbours nearly everything).
+      const uint32_t nparts = G / pt.P;
+      uint32_t nr0 = 0;
+      for (uint32_t w = pt.plane; w < W; w += pt.P) nr0 += __popc(R0[w]);
+      nr0 = __reduce_add_sync(pt.pmask, nr0);
+      const uint32_t L = (nparts == 1u || nr0 >= 4u * nparts) ? 1u : (nr0 <= 2u ? 3u : 2u);
+      const bool top_owner = part == 0u;
+      auto ticket = [&]() -> uint32_t {
+        uint32_t t = 0;
+        if (pt.plane == 0) t = atomicAdd(&hdr[1], 1u);
+        return __shfl_sync(pt.pmask, t, pt.pbase);
+      };
+      uint32_t seen = 0, mine = ticket();
+      auto claim = [&]() -> bool {  // at a depth-L node: does this partition take it?
+        const bool take = seen == mine;
+        ++seen;
+        if (take) mine = ticket();
+        return take;
+      };
+
+      for (uint32_t v = 0; v < d; ++v) {
         if (budgeted && over_budget()) break;
-        uint32_t v = 0;
-        if (pt.plane == 0) v = atomicAdd(&hdr[1], 1u);
-        v = __shfl_sync(pt.pmask, v, pt.pbase);
-        if (v >= d) break;
         if (!((R0[v >> 5] >> (v & 31u)) & 1u)) continue;
+        if (L == 1u && !claim()) continue;
+        const bool own1 = L == 1u || top_owner;
         const uint32_t hold = hold0 + (v != p0 ? 1u : 0u), drop = (v == p0) ? 1u : 0u;
-        st_nodes++;
+        if (own1) st_nodes++;
         if (hold > k) continue;
         uint32_t* F0 = frames;
-        for (uint32_t w = pt.plane; w < W; w += pt.P) F0[w] = B[v * W + w] & ~(R0[w] & low_mask(v, w));
+        for (uint32_t w = pt.plane; w < W; w += pt.P) F0[w] = B[v * Ws + w] & ~(R0[w] & low_mask(v, w));
         __syncwarp(pt.pmask);
-        if (!enter(F0, hold, drop)) continue;
+        if (!enter(F0, hold, drop, own1)) continue;
         int lv = 0;
         while (lv >= 0) {
           if (budgeted && over_budget()) break;
           uint32_t* F = frames + (size_t)lv * p.fw;
           uint32_t wi = 0;
           const int vb = part_next_bit(F + W, F[2 * W + 3], W, pt, &wi);
-          if (vb < 0) { --lv; continue; }
-          const uint32_t u = (uint32_t)vb;
           const uint32_t fh = F[2 * W], fd = F[2 * W + 1], fp = F[2 * W + 2];
+          if (vb < 0) {
+            // every other branch is done: the pivot's branch replaces the frame
+            const bool own = (uint32_t)lv + 1u >= L || top_owner;
+            if (own) st_nodes++;
+            for (uint32_t w = pt.plane; w < W; w += pt.P) F[w] &= B[fp * Ws + w];
+            __syncwarp(pt.pmask);
+            if (!enter(F, fh, fd + 1u, own)) --lv;
+            continue;
+          }
+          const uint32_t u = (uint32_t)vb;
           __syncwarp(pt.pmask);
           if (pt.plane == 0) {
             F[W + wi] &= ~(1u << (u & 31u));
             F[2 * W + 3] = wi;
           }
-          const uint32_t h2 = fh + (u != fp ? 1u : 0u), d2 = fd + (u == fp ? 1u : 0u);
-          st_nodes++;
+          const uint32_t h2 = fh + 1u;  // u is not the pivot
           bool descend = h2 <= k;
           if (descend && (uint32_t)(lv + 1) >= p.depth) {
             if (pt.plane == 0) set_error(p.err, DEV_ERR_STACK);
             descend = false;
           }
+          bool own = (uint32_t)lv + 2u > L || top_owner;
+          if (descend && (uint32_t)lv + 2u == L) own = descend = claim();
+          if (own) st_nodes++;
           uint32_t* Fc = F + p.fw;
           if (descend)
-            for (uint32_t w = pt.plane; w < W; w += pt.P) Fc[w] = F[w] & B[u * W + w];
+            for (uint32_t w = pt.plane; w < W; w += pt.P) Fc[w] = F[w] & B[u * Ws + w];
           __syncwarp(pt.pmask);
           if (pt.plane == 0) F[u >> 5] &= ~(1u << (u & 31u));  // later siblings exclude u
           __syncwarp(pt.pmask);
-          if (descend && enter(Fc, h2, d2)) ++lv;
+          if (descend && enter(Fc, h2, fd, own)) ++lv;
         }
       }
     }
@@ -615,6 +693,13 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
     P = 1;
     W = W <= 1 ? 1 : (W <= 2 ? 2 : 4);
   }
+  // Pivoting walks each clique-tree node with a whole warp (partitions of one
+  // warp would walk different nodes one after another); the partition size
+  // is the number of lanes that score one pivot candidate.
+  if (lp.mode != KC_MODE_ORIENT) {
+    p.Q = lp.q;
+    P = 32;
+  }
   const uint32_t nparts = G / P;
   const uint32_t gpb = block / G;
   uint32_t depth, fw;
@@ -622,13 +707,18 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
     depth = std::max<uint32_t>(1, t_max >= 2 ? t_max - 2 : 1);
     fw = W + 1;
   } else {
-    depth = lp.depth_boost ? dcap + 2 : std::min<uint32_t>(dcap + 2, 64);
+    // a pushed frame holds one more vertex than its parent (pivot branches
+    // reuse the parent's slot), so k - hold0 + 1 levels always suffice
+    const uint32_t hold0 = lp.edge ? 2u : 1u;
+    depth = std::min<uint32_t>(dcap + 2, std::max<uint32_t>(2, lp.k_max + 2 - std::min(lp.k_max, hold0)));
     fw = 2 * W + 4;
   }
   auto al4 = [](size_t x) { return (x + 3) & ~(size_t)3; };
   const size_t hdr = 16, sS = al4(dcap), sR0 = al4(W);
-  const size_t sB = (size_t)dcap * W;
-  const size_t sFr = lane ? 0 : al4((size_t)nparts * depth * fw);
+  const bool pivot = lp.mode != KC_MODE_ORIENT;
+  const size_t sB = (size_t)dcap * (pivot ? (W | 1u) : W);  // pivot rows use an odd stride
+  const size_t pstride = (size_t)depth * fw + (pivot ? al4(dcap) : 0);
+  const size_t sFr = lane ? 0 : al4((size_t)nparts * pstride);
   const size_t limit_words = (size_t)ctx->max_smem_optin / 4;
   // hash of S for the bitmap build: 2*hT words, hT the power of two >= 2 dcap
   // (>= 4 dcap for warp units, whose mostly-missing lookups then probe ~1.4 slots)
@@ -639,8 +729,10 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
   }
   bool bitmap_global = lp.force_global_bitmap;
   bool frames_global = false;
+  // The hash is needed only while the bitmap is built and the frames only
+  // after it, so in shared memory they share one region.
   auto group_words = [&]() {
-    return hdr + sS + sR0 + 2 * (size_t)hT + (bitmap_global ? 0 : al4(sB)) + (frames_global ? 0 : sFr);
+    return hdr + sS + sR0 + (bitmap_global ? 0 : al4(sB)) + std::max<size_t>(frames_global ? 0 : sFr, 2 * (size_t)hT);
   };
   if ((size_t)gpb * group_words() > limit_words) frames_global = true;
   if ((size_t)gpb * group_words() > limit_words) bitmap_global = true;
@@ -653,13 +745,14 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
   p.G = G;
   p.depth = depth;
   p.fw = fw;
+  p.pstride = (uint32_t)pstride;
   p.group_words = (uint32_t)group_words();
   p.off_R0 = (uint32_t)(hdr + sS);
-  p.off_H = (uint32_t)(hdr + sS + sR0);
   p.hash_T = hT;
   p.lane_dfs = lane ? 1u : 0u;
-  p.off_B = (uint32_t)(hdr + sS + sR0 + 2 * (size_t)hT);
+  p.off_B = (uint32_t)(hdr + sS + sR0);
   p.off_fr = (uint32_t)(p.off_B + (bitmap_global ? 0 : al4(sB)));
+  p.off_H = p.off_fr;
   p.bitmap_global = bitmap_global;
   p.frames_global = frames_global;
   p.gbuf_words = (bitmap_global ? al4(sB) : 0) + (frames_global ? sFr : 0);

@@ -18,6 +18,7 @@ struct CountParams {
   uint32_t cls;              // this launch's class
   uint32_t n_units_max;      // host upper bound on the class size (grid sizing)
   uint32_t edge_units;       // 0 node units, 1 edge units
+  uint32_t edge_roots;       // node units whose root branches are their out-edges (edge units grouped by source)
   const uint32_t* vgraph;    // graph of every rank label, or null
   const uint32_t* gk;        // k of every graph, or null
   uint32_t k0;               // k when gk is null
@@ -30,6 +31,8 @@ struct CountParams {
   uint32_t G;                // threads per unit group (32 or blockDim.x)
   uint32_t depth;            // traversal stack frames per partition
   uint32_t fw;               // words per frame
+  uint32_t pstride;          // words per partition: depth frames, then (pivoting) a candidate list of dcap
+  uint32_t Q;                // pivoting: lanes that score one candidate (0 = chosen per node)
   uint32_t group_words;      // shared-memory words per group
   uint32_t off_B, off_R0, off_fr;  // shared-memory offsets (words) inside a group
   uint32_t off_H;            // shared-memory offset of the hash of S (keys, then local indices)
@@ -49,6 +52,7 @@ struct CountParams {
 
 struct LaunchPlan {
   uint32_t mode = 0, encoding = 0, part = 0;
+  uint32_t q = 0;  // pivoting: lanes per candidate score (the request's partition size, 0 = per node)
   bool edge = false;
   uint32_t dcap = 0, G = 32, block = 128;
   bool force_global_bitmap = false;
@@ -95,13 +99,21 @@ constexpr uint32_t kHeavyBounds = 40;     // [0, heavy count]
 struct CountPlan {
   kc_graph* g = nullptr;
   CountRequest req;
-  bool edge = false;
+  bool edge = false;        // one unit per DAG edge
+  bool edge_roots = false;  // edge units grouped by source: node units, edges as root branches
   uint32_t n_units = 0, max_size = 0;
   uint32_t *size = nullptr, *hist = nullptr, *rev = nullptr, *queue = nullptr, *scratch = nullptr;
   uint32_t* heavy = nullptr;
   unsigned long long* d_out = nullptr;
   PreparedLaunch launches[kNumClasses + 1];
   bool active[kNumClasses + 1] = {false, false, false, false, false};
+  // the class launches run side by side, each on its own stream, so one
+  // class's tail overlaps the others' work; the heavy pass follows them all
+  cudaStream_t side[kNumClasses] = {};
+  cudaEvent_t fork = nullptr, join[kNumClasses] = {};
+  // per-launch timing events (single-graph calls that ask for statistics)
+  bool timed = false;
+  cudaEvent_t tbeg[kNumClasses + 1] = {}, tend[kNumClasses + 1] = {};
 };
 
 kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long* d_out, uint32_t depth_boost,

@@ -362,15 +362,15 @@ __global__ void __launch_bounds__(256) k_count_list(CountParams p, size_t cap_ed
       // A node with `hold` held vertices, `drop` pivots and candidates F[0, nc)
       // contributes sum_j C(drop, j) * cliques(G[F], r - j), r = k - hold; for
       // r <= 2 the sum is closed (1, |F| and the edges of G[F]).
-      auto enter = [&](uint32_t* F, uint32_t nc, uint32_t hold, uint32_t drop) -> bool {
+      auto enter = [&](uint32_t* F, uint32_t nc, uint32_t hold, uint32_t drop, bool own) -> bool {
         const uint32_t r = k - hold;  // callers keep hold <= k
         if (nc == 0u) {
-          acc += binom(drop, r);
+          if (own) acc += binom(drop, r);
           return false;
         }
         if (hold + drop + nc < k) return false;
         if (r <= 1u) {
-          acc += (r == 0u) ? (unsigned __int128)1u : (unsigned __int128)(nc + drop);
+          if (own) acc += (r == 0u) ? (unsigned __int128)1u : (unsigned __int128)(nc + drop);
           return false;
         }
         // lanes take candidates in turn and score each by |F ∩ N(u)|
@@ -387,16 +387,18 @@ __global__ void __launch_bounds__(256) k_count_list(CountParams p, size_t cap_ed
         }
         for (uint32_t o = 1; o < pt.P; o <<= 1) esum += __shfl_xor_sync(pt.pmask, esum, o);
         if (r == 2u) {
-          acc += (unsigned __int128)(esum / 2u) + (unsigned __int128)drop * nc + binom(drop, 2u);
-          st_words += (unsigned long long)nc * nc;
+          if (own) acc += (unsigned __int128)(esum / 2u) + (unsigned __int128)drop * nc + binom(drop, 2u);
+          if (own) st_words += (unsigned long long)nc * nc;
           return false;
         }
         best = __reduce_max_sync(pt.pmask, best);
-        st_words += (unsigned long long)nc * nc;
+        if (own) st_words += (unsigned long long)nc * nc;
         const uint32_t piv = 0xffffu - (best & 0xffffu);
         const uint32_t* Lq = row(piv);
         const uint32_t lq = rowlen(piv);
-        const uint32_t rl = part_filter(F, nc, F + D, pt, [&](uint32_t x) { return !bsearch_u32(Lq, lq, x); });
+        // branches: candidates outside N(piv) less the pivot, whose branch is
+        // taken last in this frame's own slot
+        const uint32_t rl = part_filter(F, nc, F + D, pt, [&](uint32_t x) { return x != piv && !bsearch_u32(Lq, lq, x); });
         __syncwarp(pt.pmask);
         if (pt.plane == 0) {
           F[2 * D] = nc; F[2 * D + 1] = rl; F[2 * D + 2] = 0;
@@ -406,15 +408,35 @@ __global__ void __launch_bounds__(256) k_count_list(CountParams p, size_t cap_ed
         return true;
       };
 
-      for (;;) {
-        uint32_t v = 0;
-        if (pt.plane == 0) v = atomicAdd(&hdr[1], 1u);
-        v = __shfl_sync(pt.pmask, v, pt.pbase);
-        if (v >= d) break;
+      // Work split inside the unit, as in the bitmap kernel: the tree is cut
+      // at depth L, nodes at depth L go out by ticket (hdr[1]), every
+      // partition walks the levels above the cut, partition 0 alone counts them.
+      const uint32_t nparts = G / pt.P;
+      uint32_t nr0 = 0;
+      for (uint32_t v = pt.plane; v < d; v += pt.P) nr0 += (v == p0 || !bsearch_u32(Lp0, lp0, v)) ? 1u : 0u;
+      nr0 = __reduce_add_sync(pt.pmask, nr0);
+      const uint32_t L = (nparts == 1u || nr0 >= 4u * nparts) ? 1u : (nr0 <= 2u ? 3u : 2u);
+      const bool top_owner = part == 0u;
+      auto ticket = [&]() -> uint32_t {
+        uint32_t t = 0;
+        if (pt.plane == 0) t = atomicAdd(&hdr[1], 1u);
+        return __shfl_sync(pt.pmask, t, pt.pbase);
+      };
+      uint32_t seen = 0, mine = ticket();
+      auto claim = [&]() -> bool {
+        const bool take = seen == mine;
+        ++seen;
+        if (take) mine = ticket();
+        return take;
+      };
+
+      for (uint32_t v = 0; v < d; ++v) {
         // root branches: vertices not adjacent to the root pivot (p0 included)
         if (v != p0 && bsearch_u32(Lp0, lp0, v)) continue;
+        if (L == 1u && !claim()) continue;
+        const bool own1 = L == 1u || top_owner;
         const uint32_t hold = hold0 + (v != p0 ? 1u : 0u), drop = (v == p0) ? 1u : 0u;
-        st_nodes++;
+        if (own1) st_nodes++;
         if (hold > k) continue;
         // child: N(v) minus the earlier root branches (indices < v not adjacent to p0)
         const uint32_t* Lv = row(v);
@@ -424,23 +446,37 @@ __global__ void __launch_bounds__(256) k_count_list(CountParams p, size_t cap_ed
           return !(x < v && (x == p0 || !bsearch_u32(Lp0, lp0, x)));
         });
         __syncwarp(pt.pmask);
-        if (!enter(F0, nc, hold, drop)) continue;
+        if (!enter(F0, nc, hold, drop, own1)) continue;
         int lv = 0;
         while (lv >= 0) {
           uint32_t* F = frames + (size_t)lv * p.fw;
           const uint32_t clen = F[2 * D], rlen = F[2 * D + 1], rcur = F[2 * D + 2];
-          if (rcur >= rlen) { --lv; continue; }
-          const uint32_t u = F[D + rcur];
           const uint32_t fh = F[2 * D + 3], fd = F[2 * D + 4], fp = F[2 * D + 5];
           __syncwarp(pt.pmask);
+          if (rcur >= rlen) {
+            // every other branch is done: the pivot's branch, C ∩ N(piv)
+            // (disjoint from the branches), replaces the frame in place
+            const bool own = (uint32_t)lv + 1u >= L || top_owner;
+            if (own) st_nodes++;
+            const uint32_t* Lq = row(fp);
+            const uint32_t lq = rowlen(fp);
+            const uint32_t nc = part_filter(F, clen, F, pt, [&](uint32_t x) { return bsearch_u32(Lq, lq, x); });
+            __syncwarp(pt.pmask);
+            if (!enter(F, nc, fh, fd + 1u, own)) --lv;
+            continue;
+          }
+          const uint32_t u = F[D + rcur];
+          __syncwarp(pt.pmask);
           if (pt.plane == 0) F[2 * D + 2] = rcur + 1;
-          const uint32_t h2 = fh + (u != fp ? 1u : 0u), d2 = fd + (u == fp ? 1u : 0u);
-          st_nodes++;
+          const uint32_t h2 = fh + 1u;  // u is not the pivot
           bool descend = h2 <= k;
           if (descend && (uint32_t)(lv + 1) >= p.depth) {
             if (pt.plane == 0) set_error(p.err, DEV_ERR_STACK);
             descend = false;
           }
+          bool own = (uint32_t)lv + 2u > L || top_owner;
+          if (descend && (uint32_t)lv + 2u == L) own = descend = claim();
+          if (own) st_nodes++;
           if (descend) {
             // child = C ∩ N(u) minus the earlier branches R[0, rcur)
             const uint32_t* Lu = row(u);
@@ -451,7 +487,7 @@ __global__ void __launch_bounds__(256) k_count_list(CountParams p, size_t cap_ed
               return bsearch_u32(Lu, lu, x) && !(x < u && bsearch_u32(Rl, rcur, x));
             });
             __syncwarp(pt.pmask);
-            if (enter(Fc, nc, h2, d2)) ++lv;
+            if (enter(Fc, nc, h2, fd, own)) ++lv;
           }
           __syncwarp(pt.pmask);
         }
@@ -485,7 +521,9 @@ kc_status prepare_launch_list(kc_ctx* ctx, const LaunchPlan& lp, const CountPara
     depth = std::max<uint32_t>(1, t >= 2 ? t - 2 : 1);
     fw = D + 2;
   } else {
-    depth = lp.depth_boost ? D + 2 : std::min<uint32_t>(D + 2, 64);
+    // pivot branches reuse their parent's slot: k - hold0 + 1 levels suffice
+    const uint32_t hold0 = lp.edge ? 2u : 1u;
+    depth = std::min<uint32_t>(D + 2, std::max<uint32_t>(2, lp.k_max + 2 - std::min(lp.k_max, hold0)));
     fw = 2 * D + 6;
   }
   const size_t full_edges = lp.mode == KC_MODE_ORIENT ? (size_t)D * (D - 1) / 2 : (size_t)D * (D - 1);
