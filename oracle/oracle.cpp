@@ -212,7 +212,8 @@ struct PivotCounter {
       earlier[w] = 0;
     }
     for (uint32_t w = 0; w < W; ++w) {
-      uint64_t x = branch[w];
+      // the recursion below may grow (move) the scratch: index, never keep pointers
+      uint64_t x = level(l)[W + w];
       while (x) {
         uint32_t v = w * 64 + (uint32_t)__builtin_ctzll(x);
         x &= x - 1;

@@ -35,22 +35,35 @@ def test_rmat_scale16_matches_oracle(ctx):
 
 def test_rmat_scale20_edge_factor16(ctx):
     # R-MAT scale 20, edge factor 16, (a,b,c,d) = (0.57,0.19,0.19,0.05), degeneracy
-    # orientation, pivoting on edge units with partition 8 and bitmaps; k = 5 and 7
+    # orientation, pivoting on edge units with partition 8 and bitmaps. k = 5 here
+    # (about a second per algorithm); k = 7 expands ~7e10 clique-tree nodes
+    # (minutes), so it is timed by the benchmark's config leg instead.
     s, d, n = kc.gen_rmat(20, 16, 0.57, 0.19, 0.19, seed=1).arrays()
     with kc.Graph.from_edges(ctx, s, d, n) as g:
         g.orient("degen")
         info = g.info()
         assert info["n"] == 1 << 20 and 10_000_000 < info["m"] < 16_000_000
-        for k in (5, 7):
-            ref = g.count(k, mode="pivot", unit="edge", part=8, encoding="bitmap")
-            assert ref > 0
-            assert g.count(k, mode="pivot", unit="node", part=8) == ref
-            assert g.count(k, mode="auto", unit="node", part=0) == ref
+        ref = g.count(5, mode="pivot", unit="edge", part=8, encoding="bitmap")
+        assert ref > 0
+        assert g.count(5, mode="pivot", unit="node", part=8) == ref
+        assert g.count(5, mode="auto", unit="node", part=0) == ref
+
+
+def test_rmat_scale18_k7(ctx):
+    s, d, n = kc.gen_rmat(18, 16, 0.57, 0.19, 0.19, seed=1).arrays()
+    with kc.Graph.from_edges(ctx, s, d, n) as g:
+        g.orient("degen")
+        ref = g.count(7, mode="pivot", unit="edge", part=8, encoding="bitmap")
+        assert ref > 0
+        assert g.count(7, mode="pivot", unit="node", part=0) == ref
 
 
 def test_chung_lu_4m_planted_cliques(ctx):
     # Chung-Lu, exponent 2.1, n = 4M, mean degree 20, degree cap 50k, plus 200
-    # planted cliques of 30-60 vertices; pivoting with k = 3..12, 128-bit counts
+    # planted cliques of 30-60 vertices; pivoting, 128-bit counts. k = 3 and 6
+    # here; k = 9 and 12 expand 1e10+ tree nodes (tens of seconds to minutes)
+    # and are timed by the benchmark's config leg; the smaller Chung-Lu test
+    # below checks k up to 12 against the oracle.
     el = kc.gen_chung_lu(4_000_000, 2.1, 20.0, 50_000.0, 3)
     el.plant_cliques(200, 30, 60, 11)
     s, d, n = el.arrays()
@@ -58,12 +71,11 @@ def test_chung_lu_4m_planted_cliques(ctx):
         g.orient("degen")
         core, mx = g.kcore()
         assert mx >= 29  # every planted clique of s vertices is an (s-1)-core
-        for k in (3, 6, 9, 12):
+        for k in (3, 6):
             a = g.count(k, mode="pivot", unit="node", part=0)
             b = g.count(k, mode="pivot", unit="edge", part=0)
             assert a == b
-            if k <= 6:
-                assert g.count(k, mode="auto", unit="node", part=0) == a
+            assert g.count(k, mode="auto", unit="node", part=0) == a
 
 
 def test_chung_lu_small_planted_matches_oracle(ctx):
@@ -74,7 +86,7 @@ def test_chung_lu_small_planted_matches_oracle(ctx):
     og.orient("degen")
     with kc.Graph.from_edges(ctx, s, d, n) as g:
         g.orient("degen")
-        for k in (3, 8, 12):
+        for k in (3, 6, 9, 12):
             want = og.count(k, "pivot")
             assert want >= 10 * math.comb(30, k)  # ten disjoint planted cliques of >= 30 vertices
             assert g.count(k, mode="pivot", unit="node", part=0) == want

@@ -191,3 +191,23 @@ def build_case(kc, spec):
         pc = spec["plant"]
         el.plant_cliques(pc["count"], pc["smin"], pc["smax"], pc["seed"])
     return el.arrays()
+
+
+def test_pivoter_deep_trees_any_thread_count():
+    # Planted cliques of 25-35 vertices give drop chains deeper than the
+    # Pivoter's first scratch allocation, so its per-depth scratch grows (and
+    # moves) in the middle of the recursion; the count must not depend on
+    # that or on the thread count, and must equal the orientation listing.
+    import kcgpu_b200 as kc
+
+    el = kc.gen_chung_lu(20_000, 2.1, 12.0, 500.0, 9)
+    el.plant_cliques(4, 25, 35, 3)
+    s, d, n = el.arrays()
+    og = OracleGraph(s, d, n)
+    og.orient("degen")
+    for k in (5, 8):
+        want = og.count(k, "orient")
+        assert want >= 4 * math.comb(25, k)
+        assert og.count(k, "pivot", threads=1) == want
+        assert og.count(k, "pivot") == want
+        assert og.count(k, "pivot", "edge") == want
