@@ -50,7 +50,11 @@ def parse():
     ap.add_argument("--plain-sample", type=int, default=400)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="batched", choices=["batched", "serving"])
+    ap.add_argument("--workload", default="batched", choices=["batched", "serving", "rmat", "chunglu", "er"])
+    ap.add_argument("--scale", type=int, default=20, help="rmat: log2 of the vertex count")
+    ap.add_argument("--ks", default="", help="single-graph legs: comma-separated k values")
+    ap.add_argument("--unit", default="", help="single-graph legs: node|edge (default: the config's)")
+    ap.add_argument("--part", type=int, default=-1, help="single-graph legs: partition size (default: the config's)")
     ap.add_argument("--requests", type=int, default=128)
     ap.add_argument("--rate", type=float, default=2000.0)
     ap.add_argument("--serve-max-edges", type=float, default=1e5)
@@ -138,6 +142,70 @@ def run_serving(args):
             "config": {"workload": "serving: %d requests, 30%% on 8 resident graphs, degeneracy orientation, "
                                    "autotuned, 4 streams" % len(reqs)},
             "clocks": clk, "data": "synthetic (seeded generators)"}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def run_single(args):
+    """One of the single-graph configurations, counted by the plain one-graph
+    path: the graph is built and oriented once, one untimed k = 3 count warms
+    the kernels up, then each k is counted once; device time from the count
+    statistics.
+      er      : G(2000, 0.01) seed 1, degree orientation, orientation mode,
+                node units, partition 8, bitmap, k = 4
+      rmat    : R-MAT scale S, edge factor 16, (0.57, 0.19, 0.19), degeneracy,
+                pivoting, edge units, partition 8, bitmap, k = 5, 7
+      chunglu : Chung-Lu n = 4M, exponent 2.1, mean degree 20, cap 50k, 200
+                planted cliques of 30-60, degeneracy, pivoting, node units,
+                k = 3, 6, 9, 12"""
+    import torch
+
+    import kcgpu_b200 as kc
+
+    torch.cuda.set_device(0)
+    ctx = kc.Context(0)
+    if args.workload == "er":
+        el = kc.gen_er(2000, 0.01, 1)
+        orient, mode, unit, part, ks, enc = "degree", "orient", "node", 8, [4], "bitmap"
+        name = "ER G(2000, 0.01) seed 1"
+    elif args.workload == "rmat":
+        el = kc.gen_rmat(args.scale, 16, 0.57, 0.19, 0.19, seed=1)
+        orient, mode, unit, part, ks, enc = "degen", "pivot", "edge", 8, [5, 7], "bitmap"
+        name = "R-MAT scale %d, edge factor 16, (0.57,0.19,0.19,0.05), seed 1" % args.scale
+    else:
+        el = kc.gen_chung_lu(4_000_000, 2.1, 20.0, 50_000.0, 3)
+        el.plant_cliques(200, 30, 60, 11)
+        orient, mode, unit, part, ks, enc = "degen", "pivot", "node", 0, [3, 6, 9, 12], "bitmap"
+        name = "Chung-Lu n=4M, exponent 2.1, mean degree 20, cap 50k, 200 planted cliques of 30-60"
+    if args.ks:
+        ks = [int(x) for x in args.ks.split(",")]
+    if args.unit:
+        unit = args.unit
+    if args.part >= 0:
+        part = args.part
+    s, d, n = el.arrays()
+    clocks = Clocks(0)
+    with kc.Graph.from_edges(ctx, s, d, n) as g:
+        g.orient(orient)
+        info = g.info()
+        rows = []
+        g.count(3, mode=mode, unit=unit, part=part, encoding=enc)  # warm-up: loads and sizes every kernel
+        for k in ks:
+            clocks.start()
+            t0 = time.perf_counter()
+            r = g.count(k, mode=mode, unit=unit, part=part, encoding=enc, stats=True)
+            wall = time.perf_counter() - t0
+            clk = clocks.stop()
+            clocks = Clocks(0)
+            ms = r.stats["ms_total"]
+            rows.append({"k": k, "count": str(r.count), "ms": ms, "wall_ms": wall * 1e3,
+                         "kcliques_per_s": r.count / (ms / 1e3) if ms > 0 else None,
+                         "tree_nodes": r.stats["tree_nodes"], "ms_launch": r.stats["ms_launch"],
+                         "clocks": clk})
+    line = {"metric": "single-graph k-clique counts (device ms per count)", "workload": args.workload,
+            "config": {"workload": name, "n": info["n"], "m": info["m"], "max_out_degree": info["max_out_degree"],
+                       "orientation": orient, "mode": mode, "unit": unit, "part": part, "encoding": enc},
+            "results": rows, "data": "synthetic (seeded generators)"}
     print(json.dumps(line), flush=True)
     ctx.close()
 
@@ -295,6 +363,9 @@ def main():
     args = parse()
     if args.workload == "serving" and args.impl == "engine":
         run_serving(args)
+        return
+    if args.workload in ("rmat", "chunglu", "er") and args.impl == "engine":
+        run_single(args)
         return
     world, rank, local, pg = dist_setup(args.gpus)
     if args.impl == "reference":

@@ -149,19 +149,22 @@ void count_release(CountPlan* pl) {
   for (void* p : ps)
     if (p) cudaFreeAsync(p, s);
   pl->size = pl->hist = pl->rev = pl->queue = pl->scratch = pl->heavy = nullptr;
+}
+
+// The context's side streams and events, created on first use.
+static kc_status ensure_side(kc_ctx* ctx) {
+  static_assert(kc_ctx::kSide == kNumClasses, "one side stream per size class");
+  if (ctx->fork) return KC_OK;
   for (int c = 0; c < kNumClasses; ++c) {
-    if (pl->side[c]) cudaStreamDestroy(pl->side[c]);
-    if (pl->join[c]) cudaEventDestroy(pl->join[c]);
-    pl->side[c] = nullptr;
-    pl->join[c] = nullptr;
+    KC_CUDA(cudaStreamCreateWithFlags(&ctx->side[c], cudaStreamNonBlocking));
+    KC_CUDA(cudaEventCreateWithFlags(&ctx->join[c], cudaEventDisableTiming));
   }
-  if (pl->fork) cudaEventDestroy(pl->fork);
-  pl->fork = nullptr;
   for (int c = 0; c <= kNumClasses; ++c) {
-    if (pl->tbeg[c]) cudaEventDestroy(pl->tbeg[c]);
-    if (pl->tend[c]) cudaEventDestroy(pl->tend[c]);
-    pl->tbeg[c] = pl->tend[c] = nullptr;
+    KC_CUDA(cudaEventCreate(&ctx->tbeg[c]));
+    KC_CUDA(cudaEventCreate(&ctx->tend[c]));
   }
+  KC_CUDA(cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming));
+  return KC_OK;
 }
 
 // Allocates the queue and the class launches. No kernel runs; the plan can be
@@ -255,17 +258,17 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
     }
     KC_TRY(prepare_launch(ctx, lp, p, s, &pl->launches[c]));
     pl->active[c] = true;
-    if (!heavy_pass) {
-      KC_CUDA(cudaStreamCreateWithFlags(&pl->side[c], cudaStreamNonBlocking));
-      KC_CUDA(cudaEventCreateWithFlags(&pl->join[c], cudaEventDisableTiming));
-    }
   }
-  KC_CUDA(cudaEventCreateWithFlags(&pl->fork, cudaEventDisableTiming));
-  if (pl->timed)
-    for (int c = 0; c <= kNumClasses; ++c) {
-      KC_CUDA(cudaEventCreate(&pl->tbeg[c]));
-      KC_CUDA(cudaEventCreate(&pl->tend[c]));
-    }
+  KC_TRY(ensure_side(ctx));
+  for (int c = 0; c < kNumClasses; ++c) {
+    pl->side[c] = ctx->side[c];
+    pl->join[c] = ctx->join[c];
+  }
+  pl->fork = ctx->fork;
+  for (int c = 0; c <= kNumClasses; ++c) {
+    pl->tbeg[c] = ctx->tbeg[c];
+    pl->tend[c] = ctx->tend[c];
+  }
   return KC_OK;
 }
 

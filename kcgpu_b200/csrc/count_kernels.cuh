@@ -107,11 +107,12 @@ struct CountPlan {
   unsigned long long* d_out = nullptr;
   PreparedLaunch launches[kNumClasses + 1];
   bool active[kNumClasses + 1] = {false, false, false, false, false};
-  // the class launches run side by side, each on its own stream, so one
-  // class's tail overlaps the others' work; the heavy pass follows them all
+  // the class launches run side by side, each on its own stream (the
+  // context's), so one class's tail overlaps the others' work; the heavy pass
+  // follows them all
   cudaStream_t side[kNumClasses] = {};
   cudaEvent_t fork = nullptr, join[kNumClasses] = {};
-  // per-launch timing events (single-graph calls that ask for statistics)
+  // per-launch timing (single-graph calls that ask for statistics)
   bool timed = false;
   cudaEvent_t tbeg[kNumClasses + 1] = {}, tend[kNumClasses + 1] = {};
 };

@@ -209,6 +209,16 @@ kc_status kc_ctx_destroy(kc_ctx* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     if (ctx->d_binom) cudaFree(ctx->d_binom);
+    for (int c = 0; c < kc_ctx::kSide; ++c) {
+      if (ctx->side[c]) cudaStreamSynchronize(ctx->side[c]);
+      if (ctx->side[c]) cudaStreamDestroy(ctx->side[c]);
+      if (ctx->join[c]) cudaEventDestroy(ctx->join[c]);
+    }
+    for (int c = 0; c <= kc_ctx::kSide; ++c) {
+      if (ctx->tbeg[c]) cudaEventDestroy(ctx->tbeg[c]);
+      if (ctx->tend[c]) cudaEventDestroy(ctx->tend[c]);
+    }
+    if (ctx->fork) cudaEventDestroy(ctx->fork);
     cudaStreamDestroy(ctx->stream);
   }
   delete ctx;

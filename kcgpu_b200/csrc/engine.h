@@ -21,6 +21,12 @@ struct kc_ctx {
   // exact binomial table C(r, c) as (lo, hi) pairs, rows [0, brows], cols [0, bcols]
   unsigned long long* d_binom = nullptr;
   uint32_t brows = 0, bcols = 0;
+  // the counting pass's size classes run side by side on these streams
+  // (created on first use; calls on one context are serialised by mu)
+  static constexpr int kSide = 4;
+  cudaStream_t side[kSide] = {};
+  cudaEvent_t fork = nullptr, join[kSide] = {};
+  cudaEvent_t tbeg[kSide + 1] = {}, tend[kSide + 1] = {};  // per-launch timing
 };
 
 struct kc_graph {

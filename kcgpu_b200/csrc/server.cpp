@@ -7,8 +7,10 @@
 // device footprint fits in the HBM budget next to the resident graphs and the
 // requests already on the device. Requests therefore start while others are
 // still running, and their kernels overlap on the device through the workers'
-// streams. Results are exact integers, so a request's count is the same alone
-// and in any mix.
+// streams. A worker that takes a one-shot request also takes the one-shot
+// requests queued right behind it (up to 512 requests / 8M edges, within the
+// budget) and counts them in one batched call. Results are exact integers, so
+// a request's count is the same alone and in any mix.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -127,10 +129,46 @@ void execute(kc_server* s, kc_ctx* ctx, Request& r) {
   r.res.status = st;
 }
 
+// One-shot requests queued back to back are counted together: one batched
+// call (disjoint union on the device, per-graph orientation and algorithm,
+// one captured counting launch) instead of one call each.
+constexpr size_t kBatchMaxRequests = 512;
+constexpr uint64_t kBatchMaxEdges = 8u << 20;
+
+void execute_batch(kc_server* s, kc_ctx* ctx, std::vector<std::shared_ptr<Request>>& rs) {
+  std::vector<kc_batch_graph> gs(rs.size());
+  for (size_t i = 0; i < rs.size(); ++i) {
+    Request& r = *rs[i];
+    gs[i].src = r.src.data();
+    gs[i].dst = r.dst.data();
+    gs[i].n_edges = r.src.size();
+    gs[i].n_nodes = r.n;
+    gs[i].k = r.k;
+  }
+  kc_batch_opts o;
+  std::memset(&o, 0, sizeof(o));
+  o.orientation = s->opts.orientation;
+  o.autotune = s->opts.autotune;
+  o.fixed = s->opts.fixed;
+  if (o.fixed.part == 0) o.fixed.part = 8;
+  o.use_graph = 1;
+  std::vector<kc_u128> counts(rs.size());
+  std::vector<kc_params> choice(rs.size());
+  const kc_status st = kc_batch_count(ctx, gs.data(), (uint32_t)gs.size(), &o, counts.data(), choice.data(), nullptr);
+  for (size_t i = 0; i < rs.size(); ++i) {
+    Request& r = *rs[i];
+    r.res.count = st == KC_OK ? counts[i] : kc_u128{0, 0};
+    r.res.params = choice[i];
+    r.res.status = st;
+    std::vector<uint32_t>().swap(r.src);
+    std::vector<uint32_t>().swap(r.dst);
+  }
+}
+
 void worker_main(kc_server* s, size_t wi) {
   kc_ctx* ctx = s->wctx[wi];
   for (;;) {
-    std::shared_ptr<Request> r;
+    std::vector<std::shared_ptr<Request>> rs;
     {
       std::unique_lock<std::mutex> l(s->mu);
       s->cv_work.wait(l, [&]() {
@@ -140,19 +178,32 @@ void worker_main(kc_server* s, size_t wi) {
         return s->inflight_bytes == 0 || s->resident_bytes + s->inflight_bytes + fp <= s->budget;
       });
       if (s->stop) return;
-      r = s->queue.front();
-      s->queue.pop_front();
-      s->inflight_bytes += r->footprint;
-      r->running = true;
-      r->res.start_ms = s->ms();
+      uint64_t edges = 0;
+      do {
+        std::shared_ptr<Request> r = s->queue.front();
+        s->queue.pop_front();
+        s->inflight_bytes += r->footprint;
+        r->running = true;
+        r->res.start_ms = s->ms();
+        edges += r->src.size();
+        rs.push_back(std::move(r));
+        if (rs.front()->graph_id) break;  // resident graphs run on their own
+      } while (!s->queue.empty() && rs.size() < kBatchMaxRequests && s->queue.front()->graph_id == 0 &&
+               s->queue.front()->k >= 3 && rs.front()->k >= 3 &&
+               edges + s->queue.front()->src.size() <= kBatchMaxEdges &&
+               s->resident_bytes + s->inflight_bytes + s->queue.front()->footprint <= s->budget);
     }
-    execute(s, ctx, *r);
+    if (rs.size() == 1) execute(s, ctx, *rs[0]);
+    else execute_batch(s, ctx, rs);
     {
       std::lock_guard<std::mutex> l(s->mu);
-      s->inflight_bytes -= r->footprint;
-      r->running = false;
-      r->done = true;
-      r->res.done_ms = s->ms();
+      const double t = s->ms();
+      for (auto& r : rs) {
+        s->inflight_bytes -= r->footprint;
+        r->running = false;
+        r->done = true;
+        r->res.done_ms = t;
+      }
     }
     s->cv_done.notify_all();
     s->cv_work.notify_all();
