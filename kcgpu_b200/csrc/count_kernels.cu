@@ -11,7 +11,20 @@
 // Pivot traversal (kckernels_pivoting.cuh:124-338): the succinct clique tree
 // with the max-neighbourhood pivot, ties to the smallest index; a leaf adds
 // C(drop, k - held) from an exact table (the reference parses doubles,
-// kclique/kclique.cuh:1694-1717).
+// kclique/kclique.cuh:1694-1717). Where this differs from the reference in
+// how, not what:
+//   * a whole warp walks one tree node (the reference walks one node per
+//     block with __syncthreads between steps); the launch's partition size is
+//     the number of lanes that score one pivot candidate, as the reference's
+//     partitions split the candidates of the block's node (:250-308);
+//   * nodes with r = k - held <= 2 are closed: 1, |C| + drop, or
+//     edges(G[C]) + drop |C| + C(drop, 2), instead of expanding their leaves;
+//   * the pivot's own branch is taken last and reuses its parent's frame, so
+//     the stack holds at most k - held0 + 1 frames;
+//   * a unit's tree is cut at depth 1, 2 or 3 and the nodes at the cut go to
+//     the unit's warps by ticket (a dense unit's root has few branches);
+//   * edge units are grouped by source when N+(u) fits a shared-memory bitmap:
+//     the unit u builds G[N+(u)] once and its out-edges are the root branches.
 #include <algorithm>
 
 #include "count_kernels.cuh"

@@ -38,6 +38,13 @@
 //   truss support    sup(u,v) = |N(u) ∩ N(v)| (no counterpart in the reference).
 //
 // Counts are exact unsigned 128-bit integers (mod 2^128).
+//
+// Parity unpinned against the reference itself: KCGPU ships no tests, golden
+// vectors or fixtures, and its CUDA build was not run. This oracle is pinned
+// by closed-form counts (tests/golden/closed_form.json: complete and complete
+// multipartite graphs), by brute-force enumeration of small graphs, and by
+// agreement of its two independent algorithms (orientation listing and the
+// Pivoter) on every test graph.
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
