@@ -80,8 +80,9 @@ typedef struct kc_params {
   uint32_t mode;       /* kc_mode */
   uint32_t unit;       /* kc_unit */
   uint32_t part;       /* partition size 1,2,4,8,16,32 (0 = auto): lanes that walk one
-                          subtree together (orientation), or lanes that score one
-                          pivot candidate while a warp walks the tree (pivoting) */
+                          subtree together (orientation), or the most lanes that
+                          score one pivot candidate while a warp walks the tree
+                          (pivoting) */
   uint32_t encoding;   /* kc_encoding */
   uint32_t flags;      /* KC_FLAG_* */
 } kc_params;

@@ -14,8 +14,8 @@
 // kclique/kclique.cuh:1694-1717). Where this differs from the reference in
 // how, not what:
 //   * a whole warp walks one tree node (the reference walks one node per
-//     block with __syncthreads between steps); the launch's partition size is
-//     the number of lanes that score one pivot candidate, as the reference's
+//     block with __syncthreads between steps); the launch's partition size
+//     bounds the lanes that score one pivot candidate, as the reference's
 //     partitions split the candidates of the block's node (:250-308);
 //   * nodes with r = k - held <= 2 are closed: 1, |C| + drop, or
 //     edges(G[C]) + drop |C| + C(drop, 2), instead of expanding their leaves;
@@ -155,8 +155,10 @@ __device__ bool lane_dfs(const uint32_t* B, uint32_t d, uint32_t t, uint32_t* hd
   return ok;
 }
 
+// Register budgets: orientation fits 56 registers without spills (four
+// 256-thread CTAs per SM); pivoting needs 80 (three), spilling below that.
 template <int MODE>
-__global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
+__global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountParams p) {
   extern __shared__ __align__(16) uint32_t smem[];
   const uint32_t G = p.G;
   const uint32_t gpb = blockDim.x / G;
@@ -511,10 +513,21 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
       // the parent is needed after it), so only non-pivot branches, which
       // each hold one more vertex, deepen the stack: at most k - hold0 + 1
       // levels, whatever the length of the drop chains.
+      // With a full-warp walker and rows of at most 32 words (every launch
+      // but the one for units above 1024 vertices) lane w holds word w of a
+      // candidate set, and a ballot gives the words that hold candidates:
+      // the listing and the scoring below visit only those.
+      const bool narrow = pt.P == 32u && W <= 32u;
       auto enter = [&](uint32_t* F, uint32_t hold, uint32_t drop, bool own) -> bool {
-        uint32_t nc = 0;
-        for (uint32_t w = pt.plane; w < W; w += pt.P) nc += __popc(F[w]);
-        nc = __reduce_add_sync(pt.pmask, nc);
+        uint32_t nc = 0, nzm = 0;
+        if (narrow) {
+          const uint32_t x = pt.plane < W ? F[pt.plane] : 0u;
+          nc = __reduce_add_sync(pt.pmask, (uint32_t)__popc(x));
+          nzm = __ballot_sync(pt.pmask, x != 0u);
+        } else {
+          for (uint32_t w = pt.plane; w < W; w += pt.P) nc += __popc(F[w]);
+          nc = __reduce_add_sync(pt.pmask, nc);
+        }
         const uint32_t r = k - hold;  // callers keep hold <= k
         if (nc == 0u) {
           if (own) uacc += binom(drop, r);
@@ -530,7 +543,15 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
         // lanes take them in turn, so each lane scores ceil(nc / P) of them
         uint32_t best = 0;
         unsigned long long esum = 0;
-        {
+        if (narrow) {
+          uint32_t base = 0;
+          for (uint32_t m = nzm; m; m &= m - 1u) {
+            const uint32_t q = (uint32_t)__ffs(m) - 1u;
+            const uint32_t x = F[q];
+            if ((x >> pt.plane) & 1u) cand[base + __popc(x & ((1u << pt.plane) - 1u))] = q * 32u + pt.plane;
+            base += __popc(x);
+          }
+        } else {
           uint32_t base = 0;
           for (uint32_t q = 0; q < W; ++q) {
             const uint32_t x = F[q];
@@ -541,13 +562,13 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
           }
         }
         __syncwarp(pt.pmask);
-        // Q lanes score one candidate, each over every Q-th word: the
-        // launch's partition size, or (0) as many lanes as leave none idle
-        uint32_t Q = p.Q;
-        if (Q == 0u) {
-          Q = 1u;
-          while ((Q << 1) * nc <= pt.P && Q < W) Q <<= 1;
-        }
+        // Q lanes score one candidate, each over every Q-th word: as many as
+        // leave no lane idle (one per candidate once there are 32 of them),
+        // at most the launch's partition size
+        const uint32_t nw = narrow ? (uint32_t)__popc(nzm) : W;
+        uint32_t Q = 1u;
+        while ((Q << 1) * nc <= pt.P && Q < nw) Q <<= 1;
+        if (p.Q != 0u && Q > p.Q) Q = p.Q;
         const uint32_t qs = (uint32_t)__ffs(Q) - 1u;  // Q is a power of two
         const uint32_t ng = pt.P >> qs, gq = pt.plane >> qs, lq = pt.plane & (Q - 1u);
         for (uint32_t i0 = 0; i0 < nc; i0 += ng) {
@@ -556,7 +577,16 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
           if (i < nc) {
             u = cand[i];
             const uint32_t* Bu = B + u * Ws;
-            for (uint32_t q = lq; q < W; q += Q) c += __popc(F[q] & Bu[q]);
+            if (narrow) {
+              uint32_t j = 0;
+              for (uint32_t m = nzm; m; m &= m - 1u, ++j)
+                if ((j & (Q - 1u)) == lq) {
+                  const uint32_t q = (uint32_t)__ffs(m) - 1u;
+                  c += __popc(F[q] & Bu[q]);
+                }
+            } else {
+              for (uint32_t q = lq; q < W; q += Q) c += __popc(F[q] & Bu[q]);
+            }
           }
           for (uint32_t o = 1; o < Q; o <<= 1) c += __shfl_xor_sync(pt.pmask, c, o);
           if (i < nc && lq == 0u) {
@@ -564,7 +594,7 @@ __global__ void __launch_bounds__(256) k_count_bitmap(CountParams p) {
             best = max(best, (c << 16) | (0xffffu - u));
           }
         }
-        if (own) st_words += (unsigned long long)nc * W / pt.P;
+        if (own) st_words += (unsigned long long)nc * nw / pt.P;
         for (uint32_t o = 1; o < pt.P; o <<= 1) esum += __shfl_xor_sync(pt.pmask, esum, o);
         if (r == 2u) {  // edges of G[F] + drop * |F| + C(drop, 2)
           if (own) uacc += (unsigned __int128)(esum / 2u) + (unsigned __int128)drop * nc + binom(drop, 2u);
@@ -708,7 +738,7 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
   }
   // Pivoting walks each clique-tree node with a whole warp (partitions of one
   // warp would walk different nodes one after another); the partition size
-  // is the number of lanes that score one pivot candidate.
+  // bounds the number of lanes that score one pivot candidate.
   if (lp.mode != KC_MODE_ORIENT) {
     p.Q = lp.q;
     P = 32;

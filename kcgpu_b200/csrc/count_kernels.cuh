@@ -32,7 +32,7 @@ struct CountParams {
   uint32_t depth;            // traversal stack frames per partition
   uint32_t fw;               // words per frame
   uint32_t pstride;          // words per partition: depth frames, then (pivoting) a candidate list of dcap
-  uint32_t Q;                // pivoting: lanes that score one candidate (0 = chosen per node)
+  uint32_t Q;                // pivoting: most lanes that score one candidate (0 = no bound)
   uint32_t group_words;      // shared-memory words per group
   uint32_t off_B, off_R0, off_fr;  // shared-memory offsets (words) inside a group
   uint32_t off_H;            // shared-memory offset of the hash of S (keys, then local indices)
