@@ -79,24 +79,74 @@ __device__ __forceinline__ void load_row(const uint32_t* B, uint32_t v, uint32_t
   }
 }
 
-// Orientation traversal with one lane per second-level subtree: the candidate
-// set (NW words) lives in registers, rows come from shared memory with one
-// vector load, and a lane's stack holds only the sets of the levels above it.
+// Position of the r-th (0-based) set bit of x (x has more than r set bits).
+__device__ __forceinline__ uint32_t select_bit(uint32_t x, uint32_t r) {
+  uint32_t pos = 0;
+#pragma unroll
+  for (uint32_t w = 16; w; w >>= 1) {
+    const uint32_t lowc = __popc(x & ((1u << w) - 1u));
+    if (r >= lowc) {
+      r -= lowc;
+      x >>= w;
+      pos += w;
+    }
+  }
+  return pos;
+}
+
+// Orientation traversal with one lane per subtree: the candidate set (NW
+// words) lives in registers, rows come from shared memory with one vector
+// load, and a lane's stack holds only the sets of the levels above it.
 // Counts the t-cliques of the unit whose bitmap B has rows of stride NW.
+// Lanes take subtrees by ticket: second-level vertices j (row j), or, when
+// pre holds the exclusive prefix of the row popcounts (pre[d] = edges of
+// G[S]), the third-level pairs (j, i), i in row j, with candidates
+// row j ∩ row i: a unit's first rows are its largest, and splitting them
+// keeps one lane from holding a warp's whole tail.
 // Returns false when the unit ran over its budget (its count is then void).
 template <int NW>
-__device__ bool lane_dfs(const uint32_t* B, uint32_t d, uint32_t t, uint32_t* hdr, uint32_t budget,
-                         unsigned __int128& uacc, unsigned long long& st_nodes, unsigned long long& st_words) {
+__device__ bool lane_dfs(const uint32_t* B, uint32_t d, uint32_t t, const uint32_t* pre, uint32_t* hdr,
+                         uint32_t budget, unsigned __int128& uacc, unsigned long long& st_nodes,
+                         unsigned long long& st_words) {
   uint32_t stk[kLaneStack][NW];
   unsigned long long cnt = 0;
   uint32_t since = 0;
   bool ok = true;
+  const bool pairs = pre != nullptr;
+  const uint32_t total = pairs ? pre[d] : d;
+  t = pairs ? t - 1u : t;  // a pair's candidates complete (t-1)-cliques the same way a row's complete t-cliques
   for (;;) {
     if (budget && *(volatile uint32_t*)&hdr[5]) { ok = false; break; }
-    const uint32_t j = atomicAdd(&hdr[1], 1u);
-    if (j >= d) break;
+    const uint32_t tk = atomicAdd(&hdr[1], 1u);
+    if (tk >= total) break;
     uint32_t cur[NW];
-    load_row<NW>(B, j, cur);
+    if (pairs) {
+      uint32_t lo = 0, hi = d;  // pre[lo] <= tk < pre[hi]
+      while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (pre[mid] <= tk) lo = mid;
+        else hi = mid;
+      }
+      uint32_t rj[NW], ri[NW];
+      load_row<NW>(B, lo, rj);
+      uint32_t r = tk - pre[lo], i = 0;
+      bool found = false;
+#pragma unroll
+      for (int q = 0; q < NW; ++q) {
+        const uint32_t pc = __popc(rj[q]);
+        if (!found && r < pc) {
+          i = (uint32_t)q * 32u + select_bit(rj[q], r);
+          found = true;
+        } else if (!found) {
+          r -= pc;
+        }
+      }
+      load_row<NW>(B, i, ri);
+#pragma unroll
+      for (int q = 0; q < NW; ++q) cur[q] = rj[q] & ri[q];
+    } else {
+      load_row<NW>(B, tk, cur);
+    }
     uint32_t c = 0;
 #pragma unroll
     for (int q = 0; q < NW; ++q) c += __popc(cur[q]);
@@ -403,9 +453,31 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
       // ---- orientation traversal, one lane per subtree
       const uint32_t t = p.edge_units ? k - 2u : k - 1u;
       const uint32_t bud = budgeted ? p.budget : 0u;
-      if (W == 1u) lane_dfs<1>(B, d, t, hdr, bud, uacc, st_nodes, st_words);
-      else if (W == 2u) lane_dfs<2>(B, d, t, hdr, bud, uacc, st_nodes, st_words);
-      else lane_dfs<4>(B, d, t, hdr, bud, uacc, st_nodes, st_words);
+      // for t >= 4, the exclusive prefix of the row popcounts, in the hash
+      // region (free once the bitmap is built; 2 hT >= 8 dcap words)
+      const uint32_t* pre = nullptr;
+      if (hT != 0u && t >= 4u) {
+        uint32_t carry = 0;
+        for (uint32_t j0 = 0; j0 < d; j0 += 32u) {
+          const uint32_t j = j0 + lane;
+          uint32_t c = 0;
+          if (j < d)
+            for (uint32_t q = 0; q < W; ++q) c += __popc(B[j * W + q]);
+          uint32_t incl = c;
+          for (uint32_t o = 1; o < 32u; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+          }
+          if (j < d) hkey[j] = carry + incl - c;
+          carry += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        if (lane == 0) hkey[d] = carry;
+        __syncwarp();
+        pre = hkey;
+      }
+      if (W == 1u) lane_dfs<1>(B, d, t, pre, hdr, bud, uacc, st_nodes, st_words);
+      else if (W == 2u) lane_dfs<2>(B, d, t, pre, hdr, bud, uacc, st_nodes, st_words);
+      else lane_dfs<4>(B, d, t, pre, hdr, bud, uacc, st_nodes, st_words);
     } else if (MODE == 0) {
       // ---- orientation traversal
       const uint32_t t = p.edge_units ? k - 2u : k - 1u;
