@@ -260,7 +260,9 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup(gpus: int):
+def dist_setup(gpus: int, backend: str = "nccl"):
+    """One process per GPU (torchrun env vars); the process group is only
+    used for barriers and the max-over-ranks of the step time."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -271,13 +273,17 @@ def dist_setup(gpus: int):
         import torch.distributed as dist
 
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
         pg = dist
     return world, rank, local, pg
 
 
 def barrier(pg, device):
+    """device None: a host-only group (gloo)."""
     if pg is not None:
+        if device is None:
+            pg.barrier()
+            return
         import torch
 
         pg.barrier(device_ids=[device])
@@ -289,7 +295,7 @@ def max_over_ranks(pg, x: float, device) -> float:
         return x
     import torch
 
-    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
+    t = torch.tensor([x], dtype=torch.float64, device="cpu" if device is None else f"cuda:{device}")
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 

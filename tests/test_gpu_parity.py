@@ -246,3 +246,19 @@ def test_stats_flag(ctx):
         g.orient("degree")
         r = g.count(4, stats=True)
         assert r.stats["units"] > 0 and r.stats["tree_nodes"] > 0 and r.stats["ms_total"] > 0
+
+
+def test_units_above_1024_vertices(ctx):
+    # Complete tripartite K(600, 600, 600) under degree orientation (all
+    # degrees equal, ties by id): the first vertices have out-degree up to
+    # 1200, so their units take the launch whose bitmap and frames live in
+    # global memory. Closed form: 600^3 triangles, no 4-cliques.
+    sizes = [600, 600, 600]
+    s, d, n = G.multipartite(sizes)
+    with kc.Graph.from_edges(ctx, s, d, n) as g:
+        g.orient("degree")
+        assert g.info()["max_out_degree"] > 1024
+        for k in (3, 4):
+            want = G.multipartite_kcliques(sizes, k)
+            for mode, unit, enc in VARIANTS:
+                assert g.count(k, mode=mode, unit=unit, encoding=enc) == want, (k, mode, unit, enc)
