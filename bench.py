@@ -300,9 +300,9 @@ def max_over_ranks(pg, x: float, device) -> float:
     return float(t.item())
 
 
-def make_batch(kc, n_graphs: int, seed: int):
-    el = kc.gen_batch(n_graphs, seed, pinned=True)
-    s, d, _ = el.arrays(copy=False)  # views of the page-locked arrays
+def make_batch(kc, n_graphs: int, seed: int, pinned: bool = True):
+    el = kc.gen_batch(n_graphs, seed, pinned=pinned)
+    s, d, _ = el.arrays(copy=False)  # views of the generator's (page-locked when pinned) arrays
     off, nn, kk, fam = el.batch_meta()
     return el, s, d, off, nn, kk, fam
 
@@ -340,7 +340,7 @@ def run_reference(args, world, rank, local, pg):
 
     from oracle.oracle import max_threads
 
-    el, s, d, off, nn, kk, fam = make_batch(kc, args.graphs, args.seed)
+    el, s, d, off, nn, kk, fam = make_batch(kc, args.graphs, args.seed, pinned=False)
     modes = cpu_modes(kk, fam)
     # size one step to ~12 s of CPU work on this host
     probe, t_probe, _ = cpu_oracle_sample(s, d, off, nn, kk, modes, 3.0)
