@@ -21,7 +21,7 @@ import numpy as np
 from . import _lib
 from ._lib import KCError, KcBatchOpts, KcBatchStats, KcCountStats, KcGraphInfo, KcParams, KcU128, check
 
-__all__ = ["Context", "Graph", "KCError", "SingleGPU_Kclique", "parse_spec", "MODES", "UNITS", "ENCODINGS",
+__all__ = ["Context", "Graph", "KCError", "SingleGPU_Kclique", "SingleGPU_Kclique_Local", "parse_spec", "MODES", "UNITS", "ENCODINGS",
            "ORIENTATIONS", "EdgeList", "gen_er", "gen_rmat", "gen_chung_lu", "gen_sbm", "gen_batch",
            "batch_count", "footprint_bytes", "lib"]
 
@@ -193,6 +193,21 @@ class Graph:
             return CountResult(out.value(), vals)
         return out.value()
 
+    def count_local(self, k: int, unit="node", part: int = 8):
+        """Local counts (the reference's -m lkc): a list whose entry v is the
+        number of k-cliques containing vertex v; orientation mode, bitmaps."""
+        n = self.info()["n"]
+        p = KcParams()
+        p.k = k
+        p.mode = MODES["orient"]
+        p.unit = UNITS[unit] if isinstance(unit, str) else int(unit)
+        p.part = part
+        p.encoding = ENCODINGS["bitmap"]
+        out = (KcU128 * max(1, n))()
+        tot = KcU128()
+        check(lib().kc_count_local(self._h, C.byref(p), out, C.byref(tot)))
+        return [out[v].value() for v in range(n)]
+
     def kcore(self):
         n = self.info()["n"]
         core = np.zeros(max(1, n), np.uint32)
@@ -260,6 +275,25 @@ class SingleGPU_Kclique:
 
     def count(self):
         return self._last
+
+
+class SingleGPU_Kclique_Local:
+    """Mirror of graph::SingleGPU_Kclique_Local<uint> (kclique/kclique_local.cuh:27-639):
+    the binary orientation variants; each method returns the per-vertex
+    counts (the reference keeps them in its cpn array and prints the first 50)."""
+
+    def __init__(self, dev: int, g: Graph):
+        self.dev = dev
+        self.g = g
+        self.cpn = None
+
+    def findKclqueIncremental_node_binary_async_local(self, k, part=8):
+        self.cpn = self.g.count_local(k, unit="node", part=part)
+        return self.cpn
+
+    def findKclqueIncremental_edge_binary_async_local(self, k, part=8):
+        self.cpn = self.g.count_local(k, unit="edge", part=part)
+        return self.cpn
 
 
 # ---- synthetic inputs ---------------------------------------------------------

@@ -5,7 +5,10 @@
 mirrors ``main.cu.exe -g <file> -d <dev> -m kc -o ... -k K -p ... -q ...``
 (src/main.cu:263-588, flags parsed in include/Config.h:291-363) and prints the
 reference's ``Counter = N`` line, with the exact count instead of one that
-wraps at 2^64. ``-m kcore`` prints the maximum core (src/main.cu:248-261).
+wraps at 2^64. ``-m lkc`` prints the per-vertex counts of the first 50
+vertices as the reference's SingleGPU_Kclique_Local::show does
+(src/main.cu:590-760, orientation mode with binary encoding); ``-m kcore``
+prints the maximum core (src/main.cu:248-261).
 ``-w``, ``-s`` and ``-a`` are accepted and ignored: the engine keeps no
 windows, sorts and deduplicates any input itself, and always allocates on the
 device.
@@ -74,7 +77,7 @@ def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description="k-clique counting on one GPU (reference-compatible flags)")
     ap.add_argument("-g", required=True, help="graph file or gen:... spec")
     ap.add_argument("-d", type=int, default=0, help="CUDA device")
-    ap.add_argument("-m", default="kc", choices=["kc", "kcore"])
+    ap.add_argument("-m", default="kc", choices=["kc", "lkc", "kcore"])
     ap.add_argument("-o", default="degree", choices=["degree", "degen"])
     ap.add_argument("-k", type=int, default=4)
     ap.add_argument("-p", default="node", choices=["node", "edge"])
@@ -98,6 +101,15 @@ def main(argv=None) -> int:
     if a.m == "kcore":
         _, mx = g.kcore()
         print(f"Max core = {mx}")
+    elif a.m == "lkc":
+        spec = kc.parse_spec(a.q)
+        t2 = time.perf_counter()
+        cpn = g.count_local(a.k, unit=a.p, part=spec["part"])
+        t3 = time.perf_counter()
+        print(f"count time = {t3 - t2:.6f} s")
+        print(f"Local clique counter for the first {min(50, len(cpn))} Nodes:")
+        for v in range(min(50, len(cpn))):
+            print(f"{v}\t{cpn[v]}")
     else:
         spec = kc.parse_spec(a.q)
         mode = "pivot" if spec["mode"] == 1 else "orient"

@@ -228,6 +228,7 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
     lp.k_max = k_max;
     lp.part = req.part ? req.part : auto_part(lp.mode, (lp.dcap + 31) / 32);
     lp.q = lp.mode == KC_MODE_ORIENT ? 0u : req.part;
+    lp.local = req.d_local != nullptr;
     lp.depth_boost = depth_boost;
     CountParams p;
     std::memset(&p, 0, sizeof(p));
@@ -240,6 +241,7 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
     p.n_units_max = pl->n_units;
     p.edge_units = pl->edge ? 1 : 0;
     p.edge_roots = pl->edge_roots ? 1 : 0;
+    p.local = req.d_local;
     p.vgraph = g->vgraph;
     p.gk = req.d_graph_k;
     p.k0 = req.k;

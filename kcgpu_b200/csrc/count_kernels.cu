@@ -274,12 +274,22 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
     return __shfl_sync(pt.pmask, stop, pt.pbase) != 0u;
   };
 
+  // Local (per-vertex) counts, orientation mode: every vertex of S keeps a
+  // u64 counter in shared memory for the unit, the unit's own vertices (u,
+  // and v for an edge unit) get the unit's total; both are added to the
+  // global (lo, hi) counters when the unit commits.
+  unsigned long long* loc = reinterpret_cast<unsigned long long*>(smem + (size_t)gib * p.group_words + p.off_loc);
+  auto local_add_bits = [&](uint32_t w, uint32_t x) {  // +1 for every vertex of word w of a set
+    for (; x; x &= x - 1u) atomicAdd(&loc[w * 32u + (uint32_t)__ffs(x) - 1u], 1ull);
+  };
+
   for (;;) {
     if (gt == 0) {
       hdr[0] = atomicAdd(p.ticket, 1u);
       hdr[1] = 0;  // subtree ticket of this unit
       hdr[4] = 0;  // nodes charged to this unit
       hdr[5] = 0;  // unit over budget
+      hdr[6] = hdr[7] = 0;  // local counts: the unit's total (u64)
     }
     gsync();
     const uint32_t ui = hdr[0];
@@ -348,6 +358,15 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
       const uint32_t t = p.edge_units ? k - 2u : k - 1u;
       if (t <= 1u || d < t) {
         if (part == 0 && d >= t) acc += (t == 0u) ? 1u : d;
+        if (p.local && d >= t && d <= p.dcap) {
+          if (t == 1u)
+            for (uint32_t i = gt; i < d; i += G) atomic_add_u128(p.local + 2ull * S[i], 1u);
+          if (gt == 0) {
+            const unsigned long long tot = (t == 0u) ? 1ull : d;
+            atomic_add_u128(p.local + 2ull * src, tot);
+            if (p.edge_units) atomic_add_u128(p.local + 2ull * p.col[unit], tot);
+          }
+        }
         gsync();
         continue;
       }
@@ -363,6 +382,8 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
 
     // ---- induced subgraph on S as a bitmap (row j, bit i: S[i] in N+(S[j]))
     for (uint32_t i = gt; i < d * Ws; i += G) B[i] = 0u;
+    if (MODE == 0 && p.local)
+      for (uint32_t i = gt; i < d; i += G) loc[i] = 0ull;
     const uint32_t hshift = hT ? 33u - (uint32_t)__ffs(hT) : 0u;  // 32 - log2(hT)
     if (hT) {
       for (uint32_t i = gt; i < hT; i += G) hkey[i] = 0xffffffffu;
@@ -498,9 +519,19 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
         c = __reduce_add_sync(pt.pmask, c);
         st_nodes++;
         st_words += W - ws;
-        if (t == 2u) { uacc += c; continue; }
+        if (t == 2u) {
+          uacc += c;
+          if (p.local) {  // the edges (j, x), x in row j
+            if (pt.plane == 0 && c) atomicAdd(&loc[j], (unsigned long long)c);
+            for (uint32_t w = ws + pt.plane; w < W; w += pt.P) local_add_bits(w, F0[w]);
+          }
+          continue;
+        }
         if (c < t - 1u) continue;
-        if (pt.plane == 0) F0[W] = ws;
+        if (pt.plane == 0) {
+          F0[W] = ws;
+          if (p.local) { F0[W + 1] = j; F0[W + 2] = F0[W + 3] = 0u; }
+        }
         __syncwarp(pt.pmask);
         int lv = 0;
         while (lv >= 0) {
@@ -508,7 +539,24 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
           uint32_t* F = frames + (size_t)lv * p.fw;
           uint32_t wi = 0;
           const int vb = part_next_bit(F, F[W], W, pt, &wi);
-          if (vb < 0) { --lv; continue; }
+          if (vb < 0) {
+            if (p.local && pt.plane == 0) {
+              // the frame's subtree total belongs to its vertex and to every ancestor
+              const unsigned long long tot = ((unsigned long long)F[W + 3] << 32) | F[W + 2];
+              if (tot) {
+                atomicAdd(&loc[F[W + 1]], tot);
+                if (lv > 0) {
+                  uint32_t* Fp = F - p.fw;
+                  const unsigned long long pt2 = (((unsigned long long)Fp[W + 3] << 32) | Fp[W + 2]) + tot;
+                  Fp[W + 2] = (uint32_t)pt2;
+                  Fp[W + 3] = (uint32_t)(pt2 >> 32);
+                }
+              }
+            }
+            __syncwarp(pt.pmask);
+            --lv;
+            continue;
+          }
           const uint32_t v = (uint32_t)vb;
           __syncwarp(pt.pmask);
           if (pt.plane == 0) { F[wi] &= ~(1u << (v & 31u)); F[W] = wi; }
@@ -527,11 +575,26 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
           st_words += W - wi;
           if (rem == 1u) {
             uacc += cc;
+            if (p.local && cc) {
+              // the cliques path + v + x: v gets cc now, the path's frames
+              // their totals on the way up, each x of the child one
+              for (uint32_t w = wi + pt.plane; w < W; w += pt.P) local_add_bits(w, F[w] & B[v * W + w]);
+              if (pt.plane == 0) {
+                atomicAdd(&loc[v], (unsigned long long)cc);
+                const unsigned long long t2 = (((unsigned long long)F[W + 3] << 32) | F[W + 2]) + cc;
+                F[W + 2] = (uint32_t)t2;
+                F[W + 3] = (uint32_t)(t2 >> 32);
+              }
+              __syncwarp(pt.pmask);
+            }
           } else if (cc >= rem) {
             if (!store) {
               if (pt.plane == 0) set_error(p.err, DEV_ERR_STACK);
             } else {
-              if (pt.plane == 0) Fc[W] = wi;
+              if (pt.plane == 0) {
+                Fc[W] = wi;
+                if (p.local) { Fc[W + 1] = v; Fc[W + 2] = Fc[W + 3] = 0u; }
+              }
               __syncwarp(pt.pmask);
               ++lv;
             }
@@ -777,6 +840,19 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
       if (gt == 0) p.heavy[atomicAdd(p.heavy_count, 1u)] = unit;
     } else {
       acc += uacc;
+      if (MODE == 0 && p.local) {
+        if (pt.plane == 0 && uacc != 0) atomicAdd(reinterpret_cast<unsigned long long*>(&hdr[6]), (unsigned long long)uacc);
+        gsync();
+        for (uint32_t i = gt; i < d; i += G)
+          if (loc[i]) atomic_add_u128(p.local + 2ull * S[i], loc[i]);
+        if (gt == 0) {
+          const unsigned long long tot = *reinterpret_cast<unsigned long long*>(&hdr[6]);
+          if (tot) {
+            atomic_add_u128(p.local + 2ull * src, tot);
+            if (p.edge_units) atomic_add_u128(p.local + 2ull * p.col[unit], tot);
+          }
+        }
+      }
     }
     gsync();
   }
@@ -803,7 +879,8 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
   const uint32_t t_max = lp.edge ? (lp.k_max >= 2 ? lp.k_max - 2 : 0) : lp.k_max - 1;
   // Warp units in orientation mode run the lane-per-subtree traversal: one
   // lane is one partition, rows have 1, 2 or 4 words, no frames in shared memory.
-  const bool lane = lp.mode == KC_MODE_ORIENT && G == 32 && dcap <= 128 && t_max <= (uint32_t)kLaneStack + 2;
+  const bool lane = lp.mode == KC_MODE_ORIENT && G == 32 && dcap <= 128 && t_max <= (uint32_t)kLaneStack + 2 &&
+                    !lp.local;
   if (lane) {
     P = 1;
     W = W <= 1 ? 1 : (W <= 2 ? 2 : 4);
@@ -820,7 +897,7 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
   uint32_t depth, fw;
   if (lp.mode == KC_MODE_ORIENT) {
     depth = std::max<uint32_t>(1, t_max >= 2 ? t_max - 2 : 1);
-    fw = W + 1;
+    fw = lp.local ? W + 4 : W + 1;  // local counts: + the frame's vertex and its subtree total
   } else {
     // a pushed frame holds one more vertex than its parent (pivot branches
     // reuse the parent's slot), so k - hold0 + 1 levels always suffice
@@ -846,8 +923,10 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
   bool frames_global = false;
   // The hash is needed only while the bitmap is built and the frames only
   // after it, so in shared memory they share one region.
+  const size_t sLoc = lp.local ? al4(2 * (size_t)dcap) : 0;  // local counts: a u64 per vertex of S
   auto group_words = [&]() {
-    return hdr + sS + sR0 + (bitmap_global ? 0 : al4(sB)) + std::max<size_t>(frames_global ? 0 : sFr, 2 * (size_t)hT);
+    return hdr + sS + sR0 + (bitmap_global ? 0 : al4(sB)) + sLoc +
+           std::max<size_t>(frames_global ? 0 : sFr, 2 * (size_t)hT);
   };
   if ((size_t)gpb * group_words() > limit_words) frames_global = true;
   if ((size_t)gpb * group_words() > limit_words) bitmap_global = true;
@@ -866,7 +945,8 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
   p.hash_T = hT;
   p.lane_dfs = lane ? 1u : 0u;
   p.off_B = (uint32_t)(hdr + sS + sR0);
-  p.off_fr = (uint32_t)(p.off_B + (bitmap_global ? 0 : al4(sB)));
+  p.off_loc = (uint32_t)(p.off_B + (bitmap_global ? 0 : al4(sB)));
+  p.off_fr = (uint32_t)(p.off_loc + sLoc);
   p.off_H = p.off_fr;
   p.bitmap_global = bitmap_global;
   p.frames_global = frames_global;

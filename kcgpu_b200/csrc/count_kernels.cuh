@@ -33,6 +33,8 @@ struct CountParams {
   uint32_t fw;               // words per frame
   uint32_t pstride;          // words per partition: depth frames, then (pivoting) a candidate list of dcap
   uint32_t Q;                // pivoting: most lanes that score one candidate (0 = no bound)
+  unsigned long long* local; // local counts: (lo, hi) per rank label, or null
+  uint32_t off_loc;          // shared-memory offset of the per-vertex local counters (u64 each)
   uint32_t group_words;      // shared-memory words per group
   uint32_t off_B, off_R0, off_fr;  // shared-memory offsets (words) inside a group
   uint32_t off_H;            // shared-memory offset of the hash of S (keys, then local indices)
@@ -53,6 +55,7 @@ struct CountParams {
 struct LaunchPlan {
   uint32_t mode = 0, encoding = 0, part = 0;
   uint32_t q = 0;  // pivoting: lanes per candidate score (the request's partition size, 0 = per node)
+  bool local = false;  // per-vertex (local) counts
   bool edge = false;
   uint32_t dcap = 0, G = 32, block = 128;
   bool force_global_bitmap = false;

@@ -434,6 +434,66 @@ kc_status kc_count(kc_graph* g, const kc_params* p, kc_u128* out, kc_count_stats
   return st;
 }
 
+kc_status kc_count_local(kc_graph* g, const kc_params* p, kc_u128* per_vertex, kc_u128* total) {
+  if (!g || !p || !per_vertex) return fail(KC_ERR_INVALID_ARG, "NULL argument");
+  if (p->k < 1) return fail(KC_ERR_INVALID_ARG, "k must be >= 1");
+  if (p->mode != KC_MODE_ORIENT || p->encoding != KC_ENC_BITMAP)
+    return fail(KC_ERR_INVALID_ARG, "local counts run the orientation mode with binary encoding");
+  if (p->unit > KC_UNIT_EDGE) return fail(KC_ERR_INVALID_ARG, "unknown unit");
+  if (p->part != 0 && (p->part > 32 || (p->part & (p->part - 1))))
+    return fail(KC_ERR_INVALID_ARG, "partition size %u is not one of 1,2,4,8,16,32", p->part);
+  if (g->oriented < 0) return fail(KC_ERR_NOT_ORIENTED, "call kc_orient before kc_count_local");
+  kc::CtxLock lock(g->ctx);
+  const uint32_t n = g->n;
+  cudaStream_t s = g->ctx->stream;
+  std::vector<unsigned long long> loc(2 * (size_t)n, 0);
+  unsigned long long tot_lo = 0, tot_hi = 0;
+  if (p->k <= 2) {
+    // k = 1: every vertex once; k = 2: every vertex in deg(v) edges
+    std::vector<uint32_t> rp((size_t)n + 1, 0);
+    if (n) {
+      KC_CUDA(cudaMemcpyAsync(rp.data(), g->rp, sizeof(uint32_t) * ((size_t)n + 1), cudaMemcpyDeviceToHost, s));
+      KC_CUDA(cudaStreamSynchronize(s));
+    }
+    for (uint32_t v = 0; v < n; ++v) per_vertex[v] = {p->k == 1 ? 1ull : (unsigned long long)(rp[v + 1] - rp[v]), 0};
+    if (total) *total = {p->k == 1 ? (unsigned long long)n : (unsigned long long)g->m, 0};
+    return KC_OK;
+  }
+  unsigned long long *d_out = nullptr, *d_local = nullptr;
+  KC_CUDA(cudaMallocAsync(&d_out, 2 * sizeof(unsigned long long), s));
+  KC_CUDA(cudaMallocAsync(&d_local, 2 * sizeof(unsigned long long) * std::max<uint32_t>(1, n), s));
+  KC_CUDA(cudaMemsetAsync(d_out, 0, 2 * sizeof(unsigned long long), s));
+  KC_CUDA(cudaMemsetAsync(d_local, 0, 2 * sizeof(unsigned long long) * std::max<uint32_t>(1, n), s));
+  kc::CountRequest req;
+  req.k = p->k;
+  req.mode = KC_MODE_ORIENT;
+  req.unit = p->unit;
+  req.part = p->part;
+  req.encoding = KC_ENC_BITMAP;
+  req.flags = 0;
+  req.k_max = p->k;
+  req.d_local = d_local;
+  kc_status st = kc::count_graph(g, req, d_out, nullptr);
+  std::vector<uint32_t> rank(n);
+  unsigned long long h[2] = {0, 0};
+  if (st == KC_OK) {
+    cudaError_t e = cudaMemcpyAsync(h, d_out, sizeof(h), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && n) e = cudaMemcpyAsync(loc.data(), d_local, sizeof(unsigned long long) * 2 * n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && n) e = cudaMemcpyAsync(rank.data(), g->rank, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = kc::cuda_fail(e, "local count readback", __FILE__, __LINE__);
+  }
+  cudaFreeAsync(d_out, s);
+  cudaFreeAsync(d_local, s);
+  if (st != KC_OK) return st;
+  // counters are indexed by rank label; the caller's array by vertex id
+  for (uint32_t v = 0; v < n; ++v) per_vertex[v] = {loc[2 * (size_t)rank[v]], loc[2 * (size_t)rank[v] + 1]};
+  tot_lo = h[0];
+  tot_hi = h[1];
+  if (total) *total = {tot_lo, tot_hi};
+  return KC_OK;
+}
+
 kc_status kc_kcore(kc_graph* g, uint32_t* core, uint32_t* max_core) {
   if (!g) return fail(KC_ERR_INVALID_ARG, "graph is NULL");
   kc::CtxLock lock(g->ctx);

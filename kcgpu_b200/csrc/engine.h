@@ -78,6 +78,8 @@ struct CountRequest {
   const uint32_t* d_graph_k = nullptr;
   uint32_t n_graphs = 1;
   uint32_t k_max = 0;
+  // local counts (orientation mode): (lo, hi) per rank label, zeroed; null otherwise
+  unsigned long long* d_local = nullptr;
 };
 
 // Runs the counting stage; d_out holds n_graphs (lo, hi) pairs and must be zeroed.

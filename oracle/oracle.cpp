@@ -135,6 +135,35 @@ struct OrientCounter {
   }
 };
 
+// Local counts: every k-clique adds 1 to each of its vertices
+// (kclique/kclique_local.cuh, the reference's -m lkc). Listing from the lowest
+// vertex u over the DAG, as the orientation counter; the path is kept so
+// each found clique can credit its members.
+struct LocalLister {
+  const or_graph& g;
+  std::vector<u128>& cnt;
+  std::vector<uint32_t> path;
+  LocalLister(const or_graph& gr, std::vector<u128>& c) : g(gr), cnt(c) {}
+
+  void rec(const std::vector<uint32_t>& C, uint32_t t) {  // t more vertices from C
+    if (t == 0) {
+      for (uint32_t v : path) cnt[v] += 1;
+      return;
+    }
+    if (C.size() < t) return;
+    for (size_t i = 0; i < C.size(); ++i) {
+      const uint32_t v = C[i];
+      const uint32_t* nv = g.dcol.data() + g.drp[v];
+      const size_t dv = g.drp[v + 1] - g.drp[v];
+      std::vector<uint32_t> next(std::min(C.size(), dv));
+      next.resize(intersect(C.data(), C.size(), nv, dv, next.data()));
+      path.push_back(v);
+      rec(next, t - 1);
+      path.pop_back();
+    }
+  }
+};
+
 // ---- pivoting (succinct clique tree) on a local induced subgraph ---------
 
 struct PivotCounter {
@@ -498,6 +527,23 @@ void or_binom(uint32_t n, uint32_t r, uint64_t* lo, uint64_t* hi) {
   u128 v = binom_u128(n, r);
   *lo = (uint64_t)v;
   *hi = (uint64_t)(v >> 64);
+}
+
+// Local counts (single-threaded; test sizes): out_lo/out_hi[v] for every vertex.
+int or_count_local(const or_graph* g, uint32_t k, uint64_t* out_lo, uint64_t* out_hi) {
+  if (g->oriented < 0 || k == 0) return -1;
+  std::vector<u128> cnt(g->n, 0);
+  LocalLister L(*g, cnt);
+  for (uint32_t u = 0; u < g->n; ++u) {
+    std::vector<uint32_t> C(g->dcol.begin() + g->drp[u], g->dcol.begin() + g->drp[u + 1]);
+    L.path.assign(1, u);
+    L.rec(C, k - 1);
+  }
+  for (uint32_t v = 0; v < g->n; ++v) {
+    out_lo[v] = (uint64_t)cnt[v];
+    out_hi[v] = (uint64_t)(cnt[v] >> 64);
+  }
+  return 0;
 }
 
 int or_max_threads(void) { return omp_get_max_threads(); }

@@ -52,6 +52,8 @@ def load():
         L.or_count.restype = C.c_int
         L.or_count.argtypes = [C.c_void_p, u32, C.c_int, C.c_int, C.c_int, P(u64), P(u64)]
         L.or_truss_support.argtypes = [C.c_void_p, P(u32)]
+        L.or_count_local.restype = C.c_int
+        L.or_count_local.argtypes = [C.c_void_p, u32, P(u64), P(u64)]
         L.or_binom.argtypes = [u32, u32, P(u64), P(u64)]
         L.or_max_threads.restype = C.c_int
         _lib = L
@@ -121,6 +123,15 @@ class OracleGraph:
         if rc != 0:
             raise RuntimeError("oracle count failed (graph not oriented or k == 0)")
         return (int(hi.value) << 64) | int(lo.value)
+
+    def count_local(self, k: int) -> list:
+        """Per-vertex k-clique counts (every clique credits each of its vertices)."""
+        lo = np.zeros(max(1, self.n), np.uint64)
+        hi = np.zeros(max(1, self.n), np.uint64)
+        rc = load().or_count_local(self._h, k, lo.ctypes.data_as(P(u64)), hi.ctypes.data_as(P(u64)))
+        if rc != 0:
+            raise RuntimeError("oracle local count failed (graph not oriented or k == 0)")
+        return [(int(h) << 64) | int(l) for l, h in zip(lo[: self.n], hi[: self.n])]
 
     def truss_support(self) -> np.ndarray:
         sup = np.zeros(max(1, self.m), np.uint32)

@@ -39,3 +39,15 @@ def test_cli_counts_complete_graph(tmp_path):
                               "-o", "degen", "-k", "5", "-p", p, "-q", q], capture_output=True, text=True, check=True)
         counter = [ln for ln in out.stdout.splitlines() if ln.startswith("Counter = ")]
         assert counter == [f"Counter = {math.comb(n, 5)}"], (q, p, out.stdout)
+
+
+@pytest.mark.gpu
+def test_cli_local_counts(tmp_path):
+    n = 10
+    lines = [f"{i} {j}" for i in range(n) for j in range(i + 1, n)]
+    (tmp_path / "k10.tsv").write_text("\n".join(lines) + "\n")
+    out = subprocess.run([sys.executable, "-m", "kcgpu_b200.cli", "-g", str(tmp_path / "k10.tsv"), "-m", "lkc",
+                          "-o", "degree", "-k", "4", "-p", "node", "-q", "o8b"], capture_output=True, text=True,
+                         check=True)
+    rows = [ln.split("\t") for ln in out.stdout.splitlines() if "\t" in ln]
+    assert rows == [[str(v), str(math.comb(n - 1, 3))] for v in range(n)]

@@ -211,3 +211,31 @@ def test_pivoter_deep_trees_any_thread_count():
         assert og.count(k, "pivot", threads=1) == want
         assert og.count(k, "pivot") == want
         assert og.count(k, "pivot", "edge") == want
+
+
+def test_local_counts_brute_force():
+    # every k-clique credits each of its vertices: brute force on small graphs,
+    # sums equal k times the global count, complete graphs in closed form
+    rng = random.Random(5)
+    for trial in range(12):
+        n = rng.randint(1, 14)
+        p = rng.choice([0.2, 0.5, 0.8])
+        edges = [(i, j) for i in range(n) for j in range(i + 1, n) if rng.random() < p]
+        s = np.array([e[0] for e in edges], np.uint32)
+        d = np.array([e[1] for e in edges], np.uint32)
+        og = OracleGraph(s, d, n)
+        og.orient("degen" if trial % 2 else "degree")
+        adj = {(min(a, b), max(a, b)) for a, b in edges}
+        for k in (1, 2, 3, 4, 5):
+            want = [0] * n
+            for c in itertools.combinations(range(n), k):
+                if all((a, b) in adj for a, b in itertools.combinations(c, 2)):
+                    for v in c:
+                        want[v] += 1
+            got = og.count_local(k)
+            assert got == want, (trial, k)
+            assert sum(got) == k * og.count(k)
+    s, d = G.complete(9)
+    og = OracleGraph(s, d, 9)
+    og.orient("degree")
+    assert og.count_local(4) == [math.comb(8, 3)] * 9
