@@ -295,6 +295,18 @@ uint64_t kc_footprint_bytes(uint32_t n_nodes, uint64_t n_edges, uint32_t max_out
 /* ---- synthetic inputs (host) ------------------------------------------- */
 /* A host edge list owned by the library; pinned = 1 uses page-locked memory. */
 typedef struct kc_edgelist kc_edgelist;
+
+/* Graph files (graph::EdgeListFile, include/FIleReader.cuh:33-937), parsed on
+ * host threads: KC_FILE_TEXT = one edge per line "src dst [anything]" (space,
+ * tab or comma separated; '#' / '%' comment and blank lines skipped);
+ * KC_FILE_MTX = Matrix Market coordinate, 1-based; KC_FILE_BEL = 24-byte
+ * records {dst u64, src u64, weight u64} (:84-90). KC_FILE_AUTO picks by
+ * extension (.bel, .mtx, else text). Malformed lines and ids of 2^32-1 or more
+ * are KC_ERR_INVALID_ARG (with the line number). */
+typedef enum { KC_FILE_AUTO = 0, KC_FILE_TEXT = 1, KC_FILE_MTX = 2, KC_FILE_BEL = 3 } kc_file_format;
+kc_status kc_edgelist_from_file(const char* path, uint32_t format, int pinned, kc_edgelist** out);
+/* kc_edgelist_from_file + kc_graph_from_edges. */
+kc_status kc_graph_from_file(kc_ctx* ctx, const char* path, uint32_t format, kc_graph** out);
 kc_status kc_edgelist_data(const kc_edgelist* e, const uint32_t** src, const uint32_t** dst,
                            uint64_t* n_edges, uint32_t* n_nodes);
 kc_status kc_edgelist_destroy(kc_edgelist* e);

@@ -22,13 +22,14 @@ from . import _lib
 from ._lib import KCError, KcBatchOpts, KcBatchStats, KcCountStats, KcGraphInfo, KcParams, KcU128, check
 
 __all__ = ["Context", "Graph", "KCError", "SingleGPU_Kclique", "SingleGPU_Kclique_Local", "parse_spec", "MODES", "UNITS", "ENCODINGS",
-           "ORIENTATIONS", "EdgeList", "gen_er", "gen_rmat", "gen_chung_lu", "gen_sbm", "gen_batch",
+           "ORIENTATIONS", "EdgeList", "read_edgelist", "gen_er", "gen_rmat", "gen_chung_lu", "gen_sbm", "gen_batch",
            "batch_count", "footprint_bytes", "lib"]
 
 MODES = {"orient": 0, "orientation": 0, "o": 0, "pivot": 1, "pivoting": 1, "p": 1, "auto": 2}
 UNITS = {"node": 0, "edge": 1}
 ENCODINGS = {"bitmap": 0, "binary": 0, "b": 0, "list": 1, "n": 1}
 ORIENTATIONS = {"degree": 0, "degen": 1, "degeneracy": 1}
+FILE_FORMATS = {"auto": 0, "text": 1, "tsv": 1, "mtx": 2, "bel": 3}
 
 
 def lib():
@@ -102,6 +103,13 @@ class Graph:
             raise ValueError("src and dst must have the same length")
         h = C.c_void_p()
         check(lib().kc_graph_from_edges(ctx.handle, _u32p(s), _u32p(d), s.size, n_nodes, C.byref(h)))
+        return cls(ctx, h)
+
+    @classmethod
+    def from_file(cls, ctx: Context, path, format: str = "auto") -> "Graph":
+        """A graph file (text edge list, .mtx or the reference's .bel)."""
+        h = C.c_void_p()
+        check(lib().kc_graph_from_file(ctx.handle, str(path).encode(), FILE_FORMATS[format], C.byref(h)))
         return cls(ctx, h)
 
     @classmethod
@@ -358,6 +366,11 @@ def _gen(fn, *args) -> EdgeList:
     h = C.c_void_p()
     check(fn(*args, C.byref(h)))
     return EdgeList(h)
+
+
+def read_edgelist(path, format: str = "auto", pinned: bool = False) -> EdgeList:
+    """Parses a graph file on host threads (kc_edgelist_from_file)."""
+    return _gen(lib().kc_edgelist_from_file, str(path).encode(), FILE_FORMATS[format], int(pinned))
 
 
 def gen_er(n: int, p: float, seed: int, pinned: bool = False) -> EdgeList:

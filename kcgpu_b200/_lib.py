@@ -103,6 +103,8 @@ SIGNATURES = {
     "kc_footprint_bytes": (u64, [u32, u64, u32]),
     "kc_edgelist_data": (i32, [C.c_void_p, P(P(u32)), P(P(u32)), P(u64), P(u32)]),
     "kc_edgelist_destroy": (i32, [C.c_void_p]),
+    "kc_edgelist_from_file": (i32, [C.c_char_p, u32, i32, P(C.c_void_p)]),
+    "kc_graph_from_file": (i32, [C.c_void_p, C.c_char_p, u32, P(C.c_void_p)]),
     "kc_gen_er": (i32, [u32, C.c_double, u64, i32, P(C.c_void_p)]),
     "kc_gen_rmat": (i32, [u32, C.c_double, C.c_double, C.c_double, C.c_double, u64, i32, P(C.c_void_p)]),
     "kc_gen_chung_lu": (i32, [u32, C.c_double, C.c_double, C.c_double, u64, i32, P(C.c_void_p)]),

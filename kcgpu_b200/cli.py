@@ -28,15 +28,12 @@ from __future__ import annotations
 import argparse
 import sys
 import time
-from pathlib import Path
-
-import numpy as np
 
 import kcgpu_b200 as kc
 
 
 def read_graph(spec: str):
-    """Returns (src, dst, n_nodes) as uint32 arrays, n_nodes 0 = max id + 1."""
+    """Returns (src, dst, n_nodes) as uint32 arrays."""
     if spec.startswith("gen:"):
         f = spec.split(":")[1:]
         kind = f[0]
@@ -51,26 +48,7 @@ def read_graph(spec: str):
         else:
             raise SystemExit(f"unknown generator {kind!r}")
         return el.arrays()
-    path = Path(spec)
-    if path.suffix == ".bel":
-        rec = np.fromfile(path, dtype=np.uint64).reshape(-1, 3)
-        return rec[:, 1].astype(np.uint32), rec[:, 0].astype(np.uint32), 0
-    if path.suffix == ".mtx":
-        rows = []
-        with open(path) as fh:
-            header_done = False
-            for line in fh:
-                if line.startswith("%") or not line.strip():
-                    continue
-                if not header_done:  # "rows cols entries"
-                    header_done = True
-                    continue
-                a, b = line.split()[:2]
-                rows.append((int(a) - 1, int(b) - 1))
-        e = np.asarray(rows, dtype=np.uint32).reshape(-1, 2)
-        return e[:, 0].copy(), e[:, 1].copy(), 0
-    e = np.loadtxt(path, dtype=np.uint64, comments=("#", "%"), usecols=(0, 1), ndmin=2)
-    return e[:, 0].astype(np.uint32), e[:, 1].astype(np.uint32), 0
+    return kc.read_edgelist(spec).arrays()  # by extension: .bel, .mtx, else a text edge list
 
 
 def main(argv=None) -> int:

@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/kc.h"
+#include "edgelist.h"
 #include "host_common.h"
 
 namespace kc {
@@ -61,46 +62,10 @@ static uint64_t mix_seed(uint64_t seed, uint64_t stream) {
 
 }  // namespace kc
 
-struct kc_edgelist {
-  std::vector<uint32_t> vsrc, vdst;  // used when not pinned
-  uint32_t* psrc = nullptr;          // page-locked copies (when pinned)
-  uint32_t* pdst = nullptr;
-  uint64_t n_edges = 0;
-  uint32_t n_nodes = 0;
-  int pinned = 0;
-  // batch metadata (kc_gen_batch)
-  std::vector<uint64_t> edge_off;
-  std::vector<uint32_t> nn, kk, fam;
-
-  const uint32_t* src() const { return pinned ? psrc : vsrc.data(); }
-  const uint32_t* dst() const { return pinned ? pdst : vdst.data(); }
-  ~kc_edgelist() {
-    if (psrc) cudaFreeHost(psrc);
-    if (pdst) cudaFreeHost(pdst);
-  }
-};
-
 namespace {
 
 using kc::Rng;
 using kc::mix_seed;
-
-// Moves the vectors into page-locked memory when requested.
-kc_status finish(kc_edgelist* e, int pinned) {
-  e->n_edges = e->vsrc.size();
-  if (!pinned) return KC_OK;
-  size_t bytes = std::max<size_t>(1, e->n_edges) * sizeof(uint32_t);
-  if (cudaMallocHost(&e->psrc, bytes) != cudaSuccess || cudaMallocHost(&e->pdst, bytes) != cudaSuccess) {
-    cudaGetLastError();
-    return kc::fail(KC_ERR_OOM, "cudaMallocHost of %zu bytes for a pinned edge list failed", bytes);
-  }
-  std::memcpy(e->psrc, e->vsrc.data(), e->n_edges * sizeof(uint32_t));
-  std::memcpy(e->pdst, e->vdst.data(), e->n_edges * sizeof(uint32_t));
-  e->pinned = 1;
-  std::vector<uint32_t>().swap(e->vsrc);
-  std::vector<uint32_t>().swap(e->vdst);
-  return KC_OK;
-}
 
 int host_threads() {
   unsigned t = std::thread::hardware_concurrency();
@@ -218,7 +183,7 @@ kc_status make(kc_edgelist** out, kc_edgelist** e) {
 }
 
 kc_status done(kc_edgelist* e, int pinned, kc_edgelist** out) {
-  kc_status st = finish(e, pinned);
+  kc_status st = kc::edgelist_finish(e, pinned);
   if (st != KC_OK) { delete e; return st; }
   *out = e;
   return KC_OK;
@@ -390,7 +355,7 @@ kc_status kc_gen_plant_cliques(kc_edgelist* e, uint32_t count, uint32_t smin, ui
     e->pinned = 0;
     e->vsrc.swap(a);
     e->vdst.swap(b);
-    return finish(e, 1);
+    return kc::edgelist_finish(e, 1);
   }
   e->vsrc.insert(e->vsrc.end(), S.begin(), S.end());
   e->vdst.insert(e->vdst.end(), D.begin(), D.end());
