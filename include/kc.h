@@ -164,12 +164,11 @@ kc_status kc_graph_get_peel(const kc_graph* g, uint32_t* priority, uint32_t* lev
 kc_status kc_count(kc_graph* g, const kc_params* p, kc_u128* out, kc_count_stats* stats);
 /* Local (per-vertex) counts, the reference's -m lkc: per_vertex[v] = number of
  * k-cliques that contain vertex v (host array of n, indexed by vertex id);
- * total (may be NULL) = the k-clique count. Orientation mode with binary
- * encoding, node or edge units, as SingleGPU_Kclique_Local::
- * findKclqueIncremental_{node,edge}_binary_async_local (kclique/kclique_local.cuh:
- * 162-340, dispatched at src/main.cu:590-760); exact 128-bit counters instead
- * of the reference's u64. The pivot variants (:342-610) are not supported here
- * (KC_ERR_INVALID_ARG). */
+ * total (may be NULL) = the k-clique count. Binary encoding (list encoding is
+ * KC_ERR_INVALID_ARG, as in the reference), orientation, pivoting or auto,
+ * node or edge units: SingleGPU_Kclique_Local::findKclqueIncremental_{node,edge}_
+ * {binary,pivot}_async_local (kclique/kclique_local.cuh:162-610, dispatched at
+ * src/main.cu:590-760), with exact 128-bit counters instead of u64. */
 kc_status kc_count_local(kc_graph* g, const kc_params* p, kc_u128* per_vertex, kc_u128* total);
 /* Parse the reference's -q spec ("o8b", "p16n", ...) into mode/part/encoding. */
 kc_status kc_parse_spec(const char* spec, kc_params* inout);

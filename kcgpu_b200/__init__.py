@@ -201,13 +201,13 @@ class Graph:
             return CountResult(out.value(), vals)
         return out.value()
 
-    def count_local(self, k: int, unit="node", part: int = 8):
+    def count_local(self, k: int, unit="node", part: int = 8, mode="orient"):
         """Local counts (the reference's -m lkc): a list whose entry v is the
-        number of k-cliques containing vertex v; orientation mode, bitmaps."""
+        number of k-cliques containing vertex v; binary encoding."""
         n = self.info()["n"]
         p = KcParams()
         p.k = k
-        p.mode = MODES["orient"]
+        p.mode = MODES[mode] if isinstance(mode, str) else int(mode)
         p.unit = UNITS[unit] if isinstance(unit, str) else int(unit)
         p.part = part
         p.encoding = ENCODINGS["bitmap"]
@@ -287,8 +287,9 @@ class SingleGPU_Kclique:
 
 class SingleGPU_Kclique_Local:
     """Mirror of graph::SingleGPU_Kclique_Local<uint> (kclique/kclique_local.cuh:27-639):
-    the binary orientation variants; each method returns the per-vertex
-    counts (the reference keeps them in its cpn array and prints the first 50)."""
+    the binary (orientation and pivot) variants; each method returns the
+    per-vertex counts (the reference keeps them in its cpn array and prints
+    the first 50)."""
 
     def __init__(self, dev: int, g: Graph):
         self.dev = dev
@@ -301,6 +302,14 @@ class SingleGPU_Kclique_Local:
 
     def findKclqueIncremental_edge_binary_async_local(self, k, part=8):
         self.cpn = self.g.count_local(k, unit="edge", part=part)
+        return self.cpn
+
+    def findKclqueIncremental_node_pivot_async_local(self, k, part=8):
+        self.cpn = self.g.count_local(k, unit="node", part=part, mode="pivot")
+        return self.cpn
+
+    def findKclqueIncremental_edge_pivot_async_local(self, k, part=8):
+        self.cpn = self.g.count_local(k, unit="edge", part=part, mode="pivot")
         return self.cpn
 
 

@@ -7,7 +7,7 @@ mirrors ``main.cu.exe -g <file> -d <dev> -m kc -o ... -k K -p ... -q ...``
 reference's ``Counter = N`` line, with the exact count instead of one that
 wraps at 2^64. ``-m lkc`` prints the per-vertex counts of the first 50
 vertices as the reference's SingleGPU_Kclique_Local::show does
-(src/main.cu:590-760, orientation mode with binary encoding); ``-m kcore``
+(src/main.cu:590-760, binary encoding); ``-m kcore``
 prints the maximum core (src/main.cu:248-261).
 ``-w``, ``-s`` and ``-a`` are accepted and ignored: the engine keeps no
 windows, sorts and deduplicates any input itself, and always allocates on the
@@ -82,7 +82,7 @@ def main(argv=None) -> int:
     elif a.m == "lkc":
         spec = kc.parse_spec(a.q)
         t2 = time.perf_counter()
-        cpn = g.count_local(a.k, unit=a.p, part=spec["part"])
+        cpn = g.count_local(a.k, unit=a.p, part=spec["part"], mode="pivot" if spec["mode"] == 1 else "orient")
         t3 = time.perf_counter()
         print(f"count time = {t3 - t2:.6f} s")
         print(f"Local clique counter for the first {min(50, len(cpn))} Nodes:")

@@ -207,7 +207,7 @@ __device__ bool lane_dfs(const uint32_t* B, uint32_t d, uint32_t t, const uint32
 
 // Register budgets: orientation fits 56 registers without spills (four
 // 256-thread CTAs per SM); pivoting needs 80 (three), spilling below that.
-template <int MODE>
+template <int MODE, bool LOCAL>
 __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountParams p) {
   extern __shared__ __align__(16) uint32_t smem[];
   const uint32_t G = p.G;
@@ -282,6 +282,8 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
   auto local_add_bits = [&](uint32_t w, uint32_t x) {  // +1 for every vertex of word w of a set
     for (; x; x &= x - 1u) atomicAdd(&loc[w * 32u + (uint32_t)__ffs(x) - 1u], 1ull);
   };
+  // pivoting keeps a (lo, hi) pair per vertex of S (counts of large cliques pass 2^64)
+  auto loc2_add = [&](uint32_t i, unsigned __int128 v) { atomic_add_u128(loc + 2ull * i, v); };
 
   for (;;) {
     if (gt == 0) {
@@ -289,7 +291,6 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
       hdr[1] = 0;  // subtree ticket of this unit
       hdr[4] = 0;  // nodes charged to this unit
       hdr[5] = 0;  // unit over budget
-      hdr[6] = hdr[7] = 0;  // local counts: the unit's total (u64)
     }
     gsync();
     const uint32_t ui = hdr[0];
@@ -358,7 +359,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
       const uint32_t t = p.edge_units ? k - 2u : k - 1u;
       if (t <= 1u || d < t) {
         if (part == 0 && d >= t) acc += (t == 0u) ? 1u : d;
-        if (p.local && d >= t && d <= p.dcap) {
+        if (LOCAL && d >= t && d <= p.dcap) {
           if (t == 1u)
             for (uint32_t i = gt; i < d; i += G) atomic_add_u128(p.local + 2ull * S[i], 1u);
           if (gt == 0) {
@@ -375,6 +376,15 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
       const uint32_t hold0 = p.edge_units ? 2u : 1u;
       if (d == 0u || hold0 + d < k || k <= hold0 + 1u) {
         if (part == 0 && k >= hold0 && hold0 + d >= k) acc += (k == hold0) ? 1u : d;
+        if (LOCAL && k >= hold0 && hold0 + d >= k && d <= p.dcap) {
+          if (k == hold0 + 1u)
+            for (uint32_t i = gt; i < d; i += G) atomic_add_u128(p.local + 2ull * S[i], 1u);
+          if (gt == 0) {
+            const unsigned long long tot = (k == hold0) ? 1ull : d;
+            atomic_add_u128(p.local + 2ull * src, tot);
+            if (p.edge_units) atomic_add_u128(p.local + 2ull * p.col[unit], tot);
+          }
+        }
         gsync();
         continue;
       }
@@ -382,8 +392,8 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
 
     // ---- induced subgraph on S as a bitmap (row j, bit i: S[i] in N+(S[j]))
     for (uint32_t i = gt; i < d * Ws; i += G) B[i] = 0u;
-    if (MODE == 0 && p.local)
-      for (uint32_t i = gt; i < d; i += G) loc[i] = 0ull;
+    if (LOCAL)
+      for (uint32_t i = gt; i < (MODE == 0 ? d : 2u * d); i += G) loc[i] = 0ull;
     const uint32_t hshift = hT ? 33u - (uint32_t)__ffs(hT) : 0u;  // 32 - log2(hT)
     if (hT) {
       for (uint32_t i = gt; i < hT; i += G) hkey[i] = 0xffffffffu;
@@ -458,13 +468,22 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
     gsync();
 
     if (MODE == 1 && k == (p.edge_units ? 4u : 3u)) {
-      // k - hold0 = 2: the unit's count is the number of edges of G[S]
+      // k - hold0 = 2: the unit's count is the number of edges of G[S]; a
+      // vertex of S is in as many of those cliques as it has neighbours in S
       if (part == 0) {
         unsigned long long e2 = 0;  // twice the edges: the bitmap is symmetric
-        for (uint32_t j = pt.plane; j < d; j += pt.P)
-          for (uint32_t w = 0; w < W; ++w) e2 += __popc(B[j * Ws + w]);
+        for (uint32_t j = pt.plane; j < d; j += pt.P) {
+          uint32_t dj = 0;
+          for (uint32_t w = 0; w < W; ++w) dj += __popc(B[j * Ws + w]);
+          e2 += dj;
+          if (LOCAL && dj) atomic_add_u128(p.local + 2ull * S[j], dj);
+        }
         for (uint32_t o = 1; o < pt.P; o <<= 1) e2 += __shfl_xor_sync(pt.pmask, e2, o);
         acc += e2 / 2u;
+        if (LOCAL && pt.plane == 0 && e2) {
+          atomic_add_u128(p.local + 2ull * src, e2 / 2u);
+          if (p.edge_units) atomic_add_u128(p.local + 2ull * p.col[unit], e2 / 2u);
+        }
       }
       gsync();
       continue;
@@ -521,7 +540,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
         st_words += W - ws;
         if (t == 2u) {
           uacc += c;
-          if (p.local) {  // the edges (j, x), x in row j
+          if (LOCAL) {  // the edges (j, x), x in row j
             if (pt.plane == 0 && c) atomicAdd(&loc[j], (unsigned long long)c);
             for (uint32_t w = ws + pt.plane; w < W; w += pt.P) local_add_bits(w, F0[w]);
           }
@@ -530,7 +549,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
         if (c < t - 1u) continue;
         if (pt.plane == 0) {
           F0[W] = ws;
-          if (p.local) { F0[W + 1] = j; F0[W + 2] = F0[W + 3] = 0u; }
+          if (LOCAL) { F0[W + 1] = j; F0[W + 2] = F0[W + 3] = 0u; }
         }
         __syncwarp(pt.pmask);
         int lv = 0;
@@ -540,7 +559,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
           uint32_t wi = 0;
           const int vb = part_next_bit(F, F[W], W, pt, &wi);
           if (vb < 0) {
-            if (p.local && pt.plane == 0) {
+            if (LOCAL && pt.plane == 0) {
               // the frame's subtree total belongs to its vertex and to every ancestor
               const unsigned long long tot = ((unsigned long long)F[W + 3] << 32) | F[W + 2];
               if (tot) {
@@ -575,7 +594,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
           st_words += W - wi;
           if (rem == 1u) {
             uacc += cc;
-            if (p.local && cc) {
+            if (LOCAL && cc) {
               // the cliques path + v + x: v gets cc now, the path's frames
               // their totals on the way up, each x of the child one
               for (uint32_t w = wi + pt.plane; w < W; w += pt.P) local_add_bits(w, F[w] & B[v * W + w]);
@@ -593,7 +612,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
             } else {
               if (pt.plane == 0) {
                 Fc[W] = wi;
-                if (p.local) { Fc[W + 1] = v; Fc[W + 2] = Fc[W + 3] = 0u; }
+                if (LOCAL) { Fc[W + 1] = v; Fc[W + 2] = Fc[W + 3] = 0u; }
               }
               __syncwarp(pt.pmask);
               ++lv;
@@ -653,6 +672,8 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
       // candidate set, and a ballot gives the words that hold candidates:
       // the listing and the scoring below visit only those.
       const bool narrow = pt.P == 32u && W <= 32u;
+      const bool lc = LOCAL;  // local (per-vertex) counts
+      unsigned __int128 leaf_cnt = 0, leaf_pinc = 0;
       auto enter = [&](uint32_t* F, uint32_t hold, uint32_t drop, bool own) -> bool {
         uint32_t nc = 0, nzm = 0;
         if (narrow) {
@@ -664,13 +685,25 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
           nc = __reduce_add_sync(pt.pmask, nc);
         }
         const uint32_t r = k - hold;  // callers keep hold <= k
+        // a node that ends here leaves (for local counts) leaf_cnt, its
+        // cliques (each holds the node's held vertices), and leaf_pinc, the
+        // cliques that hold any one of its pivots
+        leaf_cnt = 0;
+        leaf_pinc = 0;
         if (nc == 0u) {
-          if (own) uacc += binom(drop, r);
+          leaf_cnt = binom(drop, r);
+          if (r >= 1u && drop >= 1u) leaf_pinc = binom(drop - 1u, r - 1u);
+          if (own) uacc += leaf_cnt;
           return false;
         }
         if (hold + drop + nc < k) return false;
         if (r <= 1u) {
-          if (own) uacc += (r == 0u) ? (unsigned __int128)1u : (unsigned __int128)(nc + drop);
+          leaf_cnt = (r == 0u) ? (unsigned __int128)1u : (unsigned __int128)(nc + drop);
+          leaf_pinc = (r == 1u && drop >= 1u) ? 1u : 0u;
+          if (own) uacc += leaf_cnt;
+          if (lc && own && r == 1u)  // each candidate c completes one clique
+            for (uint32_t w = pt.plane; w < W; w += pt.P)
+              for (uint32_t x = F[w]; x; x &= x - 1u) loc2_add(w * 32u + (uint32_t)__ffs(x) - 1u, 1u);
           return false;
         }
         // score every candidate u by |F ∩ N(u)|: the candidates are listed
@@ -727,12 +760,16 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
           if (i < nc && lq == 0u) {
             esum += c;
             best = max(best, (c << 16) | (0xffffu - u));
+            // r = 2: candidate u is in a clique with each neighbour in F and each pivot
+            if (lc && own && r == 2u && c + drop) loc2_add(u, c + drop);
           }
         }
         if (own) st_words += (unsigned long long)nc * nw / pt.P;
         for (uint32_t o = 1; o < pt.P; o <<= 1) esum += __shfl_xor_sync(pt.pmask, esum, o);
         if (r == 2u) {  // edges of G[F] + drop * |F| + C(drop, 2)
-          if (own) uacc += (unsigned __int128)(esum / 2u) + (unsigned __int128)drop * nc + binom(drop, 2u);
+          leaf_cnt = (unsigned __int128)(esum / 2u) + (unsigned __int128)drop * nc + binom(drop, 2u);
+          leaf_pinc = drop >= 1u ? (unsigned __int128)(nc + drop - 1u) : 0u;
+          if (own) uacc += leaf_cnt;
           return false;
         }
         best = __reduce_max_sync(pt.pmask, best);
@@ -781,6 +818,50 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
         return take;
       };
 
+      // Local counts: a frame also keeps its held vertex (the branch that
+      // pushed it; none for the root pivot's branch), where its pivots start
+      // in the walker's drop list, and the totals of the cliques ended below
+      // it: T_H (each holds the frame's held vertices) and T_P (cliques that
+      // hold any one of the frame's pivots). A pivot joins the list with
+      // minus the T_P reached so far and gets the final T_P when its frame
+      // pops; totals then move up to the parent frame.
+      uint32_t* dl = cand + ((p.dcap + 3u) & ~3u);
+      uint32_t ndl = 0;
+      auto fr_get = [&](const uint32_t* F, uint32_t off) -> unsigned __int128 {
+        const uint32_t* q = F + 2u * W + off;
+        return ((unsigned __int128)q[3] << 96) | ((unsigned __int128)q[2] << 64) |
+               ((unsigned __int128)q[1] << 32) | q[0];
+      };
+      auto fr_set = [&](uint32_t* F, uint32_t off, unsigned __int128 v) {
+        uint32_t* q = F + 2u * W + off;
+        q[0] = (uint32_t)v;
+        q[1] = (uint32_t)(v >> 32);
+        q[2] = (uint32_t)(v >> 64);
+        q[3] = (uint32_t)(v >> 96);
+      };
+      auto fr_open = [&](uint32_t* F, uint32_t held) {  // plane 0
+        F[2 * W + 4] = held;
+        F[2 * W + 5] = ndl;
+        fr_set(F, 6, 0);
+        fr_set(F, 10, 0);
+      };
+      auto fr_take = [&](uint32_t* F) {  // a node that ended in this frame's slot (plane 0)
+        fr_set(F, 6, fr_get(F, 6) + leaf_cnt);
+        fr_set(F, 10, fr_get(F, 10) + leaf_pinc);
+      };
+      auto fr_close = [&](uint32_t* F, int level) {  // the frame pops (plane 0)
+        const unsigned __int128 th = fr_get(F, 6), tp = fr_get(F, 10);
+        const uint32_t hv = F[2 * W + 4], st = F[2 * W + 5];
+        if (hv != 0xffffffffu && th) loc2_add(hv, th);
+        if (tp)
+          for (uint32_t i = st; i < ndl; ++i) loc2_add(dl[i], tp);
+        if (level > 0) {
+          uint32_t* Fp = F - p.fw;
+          fr_set(Fp, 6, fr_get(Fp, 6) + th);
+          fr_set(Fp, 10, fr_get(Fp, 10) + tp);
+        }
+      };
+
       for (uint32_t v = 0; v < d; ++v) {
         if (budgeted && over_budget()) break;
         if (!((R0[v >> 5] >> (v & 31u)) & 1u)) continue;
@@ -792,7 +873,23 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
         uint32_t* F0 = frames;
         for (uint32_t w = pt.plane; w < W; w += pt.P) F0[w] = B[v * Ws + w] & ~(R0[w] & low_mask(v, w));
         __syncwarp(pt.pmask);
-        if (!enter(F0, hold, drop, own1)) continue;
+        if (!enter(F0, hold, drop, own1)) {
+          if (lc && own1 && pt.plane == 0) {
+            const unsigned __int128 x = (v != p0) ? leaf_cnt : leaf_pinc;
+            if (x) loc2_add(v, x);
+          }
+          __syncwarp(pt.pmask);
+          continue;
+        }
+        if (lc) {
+          ndl = 0;
+          if (pt.plane == 0) {
+            fr_open(F0, v != p0 ? v : 0xffffffffu);
+            if (v == p0) dl[0] = p0;  // the root pivot is a pivot of this whole subtree
+          }
+          ndl = (v == p0) ? 1u : 0u;
+          __syncwarp(pt.pmask);
+        }
         int lv = 0;
         while (lv >= 0) {
           if (budgeted && over_budget()) break;
@@ -804,9 +901,29 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
             // every other branch is done: the pivot's branch replaces the frame
             const bool own = (uint32_t)lv + 1u >= L || top_owner;
             if (own) st_nodes++;
+            __syncwarp(pt.pmask);
+            if (lc) {  // fp joins this frame's pivots
+              if (pt.plane == 0) {
+                dl[ndl] = fp;
+                const unsigned __int128 tp = fr_get(F, 10);
+                if (tp) loc2_add(fp, (unsigned __int128)0 - tp);
+              }
+              ++ndl;
+            }
             for (uint32_t w = pt.plane; w < W; w += pt.P) F[w] &= B[fp * Ws + w];
             __syncwarp(pt.pmask);
-            if (!enter(F, fh, fd + 1u, own)) --lv;
+            if (!enter(F, fh, fd + 1u, own)) {
+              if (lc) {
+                if (pt.plane == 0) {
+                  if (own) fr_take(F);
+                  fr_close(F, lv);
+                }
+                __syncwarp(pt.pmask);
+                ndl = F[2 * W + 5];
+                __syncwarp(pt.pmask);
+              }
+              --lv;
+            }
             continue;
           }
           const uint32_t u = (uint32_t)vb;
@@ -830,7 +947,20 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
           __syncwarp(pt.pmask);
           if (pt.plane == 0) F[u >> 5] &= ~(1u << (u & 31u));  // later siblings exclude u
           __syncwarp(pt.pmask);
-          if (descend && enter(Fc, h2, fd, own)) ++lv;
+          if (descend && enter(Fc, h2, fd, own)) {
+            if (lc) {
+              if (pt.plane == 0) fr_open(Fc, u);
+              __syncwarp(pt.pmask);
+            }
+            ++lv;
+          } else if (descend && lc && own) {
+            // the child ended at once: u holds its cliques, this frame takes them too
+            if (pt.plane == 0) {
+              if (leaf_cnt) loc2_add(u, leaf_cnt);
+              fr_take(F);
+            }
+            __syncwarp(pt.pmask);
+          }
         }
       }
     }
@@ -840,13 +970,21 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
       if (gt == 0) p.heavy[atomicAdd(p.heavy_count, 1u)] = unit;
     } else {
       acc += uacc;
-      if (MODE == 0 && p.local) {
-        if (pt.plane == 0 && uacc != 0) atomicAdd(reinterpret_cast<unsigned long long*>(&hdr[6]), (unsigned long long)uacc);
+      if (LOCAL) {
+        // the unit's total (its own vertices are in every one of its cliques)
+        // in hdr[8..11], free once the root pivot is known
+        unsigned long long* ut = reinterpret_cast<unsigned long long*>(&hdr[8]);
+        if (gt == 0) ut[0] = ut[1] = 0ull;
         gsync();
-        for (uint32_t i = gt; i < d; i += G)
-          if (loc[i]) atomic_add_u128(p.local + 2ull * S[i], loc[i]);
+        if (pt.plane == 0 && uacc != 0) atomic_add_u128(ut, uacc);
+        gsync();
+        for (uint32_t i = gt; i < d; i += G) {
+          const unsigned __int128 v = MODE == 0 ? (unsigned __int128)loc[i]
+                                                : (((unsigned __int128)loc[2 * i + 1] << 64) | loc[2 * i]);
+          if (v) atomic_add_u128(p.local + 2ull * S[i], v);
+        }
         if (gt == 0) {
-          const unsigned long long tot = *reinterpret_cast<unsigned long long*>(&hdr[6]);
+          const unsigned __int128 tot = ((unsigned __int128)ut[1] << 64) | ut[0];
           if (tot) {
             atomic_add_u128(p.local + 2ull * src, tot);
             if (p.edge_units) atomic_add_u128(p.local + 2ull * p.col[unit], tot);
@@ -903,13 +1041,15 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
     // reuse the parent's slot), so k - hold0 + 1 levels always suffice
     const uint32_t hold0 = lp.edge ? 2u : 1u;
     depth = std::min<uint32_t>(dcap + 2, std::max<uint32_t>(2, lp.k_max + 2 - std::min(lp.k_max, hold0)));
-    fw = 2 * W + 4;
+    fw = 2 * W + (lp.local ? 14 : 4);  // local counts: held vertex, drop-list start, two u128 totals
   }
   auto al4 = [](size_t x) { return (x + 3) & ~(size_t)3; };
   const size_t hdr = 16, sS = al4(dcap), sR0 = al4(W);
   const bool pivot = lp.mode != KC_MODE_ORIENT;
   const size_t sB = (size_t)dcap * (pivot ? (W | 1u) : W);  // pivot rows use an odd stride
-  const size_t pstride = (size_t)depth * fw + (pivot ? al4(dcap) : 0);
+  // per walker: the frames, then (pivoting) the candidate list and, for local
+  // counts, the drop list
+  const size_t pstride = (size_t)depth * fw + (pivot ? al4(dcap) * (lp.local ? 2 : 1) : 0);
   const size_t sFr = lane ? 0 : al4((size_t)nparts * pstride);
   const size_t limit_words = (size_t)ctx->max_smem_optin / 4;
   // hash of S for the bitmap build: 2*hT words, hT the power of two >= 2 dcap
@@ -923,7 +1063,8 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
   bool frames_global = false;
   // The hash is needed only while the bitmap is built and the frames only
   // after it, so in shared memory they share one region.
-  const size_t sLoc = lp.local ? al4(2 * (size_t)dcap) : 0;  // local counts: a u64 per vertex of S
+  // local counts: a u64 (orientation) or a (lo, hi) pair (pivoting) per vertex of S
+  const size_t sLoc = lp.local ? al4((pivot ? 4 : 2) * (size_t)dcap) : 0;
   auto group_words = [&]() {
     return hdr + sS + sR0 + (bitmap_global ? 0 : al4(sB)) + sLoc +
            std::max<size_t>(frames_global ? 0 : sFr, 2 * (size_t)hT);
@@ -955,7 +1096,8 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
   p.gbuf = nullptr;
 
   const size_t smem_bytes = (size_t)gpb * p.group_words * 4;
-  auto kern = lp.mode == KC_MODE_ORIENT ? k_count_bitmap<0> : k_count_bitmap<1>;
+  auto kern = lp.mode == KC_MODE_ORIENT ? (lp.local ? k_count_bitmap<0, true> : k_count_bitmap<0, false>)
+                                         : (lp.local ? k_count_bitmap<1, true> : k_count_bitmap<1, false>);
   // Several classes launch the same kernel with different shared-memory sizes;
   // the attribute is per function, so it is set to the device maximum.
   KC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->max_smem_optin));

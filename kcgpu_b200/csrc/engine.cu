@@ -437,8 +437,8 @@ kc_status kc_count(kc_graph* g, const kc_params* p, kc_u128* out, kc_count_stats
 kc_status kc_count_local(kc_graph* g, const kc_params* p, kc_u128* per_vertex, kc_u128* total) {
   if (!g || !p || !per_vertex) return fail(KC_ERR_INVALID_ARG, "NULL argument");
   if (p->k < 1) return fail(KC_ERR_INVALID_ARG, "k must be >= 1");
-  if (p->mode != KC_MODE_ORIENT || p->encoding != KC_ENC_BITMAP)
-    return fail(KC_ERR_INVALID_ARG, "local counts run the orientation mode with binary encoding");
+  if (p->mode > KC_MODE_AUTO || p->encoding != KC_ENC_BITMAP)
+    return fail(KC_ERR_INVALID_ARG, "local counts need binary encoding (as the reference's) and a known mode");
   if (p->unit > KC_UNIT_EDGE) return fail(KC_ERR_INVALID_ARG, "unknown unit");
   if (p->part != 0 && (p->part > 32 || (p->part & (p->part - 1))))
     return fail(KC_ERR_INVALID_ARG, "partition size %u is not one of 1,2,4,8,16,32", p->part);
@@ -466,7 +466,7 @@ kc_status kc_count_local(kc_graph* g, const kc_params* p, kc_u128* per_vertex, k
   KC_CUDA(cudaMemsetAsync(d_local, 0, 2 * sizeof(unsigned long long) * std::max<uint32_t>(1, n), s));
   kc::CountRequest req;
   req.k = p->k;
-  req.mode = KC_MODE_ORIENT;
+  req.mode = p->mode;
   req.unit = p->unit;
   req.part = p->part;
   req.encoding = KC_ENC_BITMAP;

@@ -31,11 +31,14 @@ def test_local_counts_match_oracle(ctx, orientation):
         og.orient(orientation)
         with kc.Graph.from_edges(ctx, s, d, n) as g:
             g.orient(orientation)
-            for k in (1, 2, 3, 4, 5, 7):
+            for k in (1, 2, 3, 4, 5, 7, 9):
                 want = og.count_local(k)
-                for unit, part in (("node", 0), ("node", 8), ("edge", 1), ("edge", 32)):
-                    got = g.count_local(k, unit=unit, part=part)
-                    assert got == want, (name, orientation, k, unit, part)
+                for mode, unit, part in (("orient", "node", 0), ("orient", "node", 8), ("orient", "edge", 1),
+                                         ("orient", "edge", 32), ("pivot", "node", 0), ("pivot", "node", 8),
+                                         ("pivot", "edge", 0), ("pivot", "edge", 2), ("auto", "node", 0),
+                                         ("auto", "edge", 0)):
+                    got = g.count_local(k, unit=unit, part=part, mode=mode)
+                    assert got == want, (name, orientation, k, mode, unit, part)
                 assert sum(want) == k * g.count(k, mode="pivot")
 
 
@@ -47,6 +50,14 @@ def test_local_counts_closed_forms(ctx):
         for k in (3, 6, 9):
             for unit in ("node", "edge"):
                 assert g.count_local(k, unit=unit) == [math.comb(n - 1, k - 1)] * n
+        for k in (12, 20, 40):  # pivoting: counts well past 2^64 per vertex at n = 130 below
+            assert g.count_local(k, mode="pivot") == [math.comb(n - 1, k - 1)] * n
+    n = 130
+    s, d = G.complete(n)
+    with kc.Graph.from_edges(ctx, s, d, n) as g:
+        g.orient("degree")
+        for unit in ("node", "edge"):
+            assert g.count_local(66, unit=unit, mode="pivot") == [math.comb(n - 1, 65)] * n
     # K(600, 600, 600): units above 1024 vertices; every vertex is in 600^2
     # triangles and no 4-clique
     sizes = [600, 600, 600]
@@ -54,8 +65,9 @@ def test_local_counts_closed_forms(ctx):
     with kc.Graph.from_edges(ctx, s, d, n) as g:
         g.orient("degree")
         for unit in ("node", "edge"):
-            assert g.count_local(3, unit=unit) == [600 * 600] * n
-            assert g.count_local(4, unit=unit) == [0] * n
+            for mode in ("orient", "pivot"):
+                assert g.count_local(3, unit=unit, mode=mode) == [600 * 600] * n
+                assert g.count_local(4, unit=unit, mode=mode) == [0] * n
 
 
 def test_local_counts_reference_mirror_and_errors(ctx):
@@ -65,10 +77,10 @@ def test_local_counts_reference_mirror_and_errors(ctx):
         ref = kc.SingleGPU_Kclique_Local(0, g)
         a = ref.findKclqueIncremental_node_binary_async_local(4, 8)
         b = ref.findKclqueIncremental_edge_binary_async_local(4, 8)
-        assert a == b and sum(a) == 4 * g.count(4)
+        c = ref.findKclqueIncremental_node_pivot_async_local(4, 8)
+        e = ref.findKclqueIncremental_edge_pivot_async_local(4, 8)
+        assert a == b == c == e and sum(a) == 4 * g.count(4)
         p = kc._lib.KcParams()
-        p.k, p.mode, p.unit, p.part, p.encoding = 4, 1, 0, 8, 0  # pivoting: not supported
+        p.k, p.mode, p.unit, p.part, p.encoding = 4, 0, 0, 8, 1  # list encoding: not supported
         out = (kc._lib.KcU128 * n)()
-        assert kc.lib().kc_count_local(g._h, kc.C.byref(p), out, None) != 0
-        p.mode, p.encoding = 0, 1  # list encoding: not supported
         assert kc.lib().kc_count_local(g._h, kc.C.byref(p), out, None) != 0
