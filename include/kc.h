@@ -125,7 +125,11 @@ kc_status kc_ctx_destroy(kc_ctx* ctx);
 /* Message for the last failing call on this host thread ("" if none). */
 const char* kc_last_error(void);
 const char* kc_status_string(kc_status s);
-/* Bounded-wait budget for device spin loops, in clock64 ticks (0 = default). */
+/* Bounded-wait budget for device spin loops, in clock64 ticks (0 = default).
+ * No kernel of this version spin-waits: work goes out by atomic tickets and the
+ * only device-wide barrier is the cooperative-launch grid sync of the peel,
+ * whose loop is bounded by the vertex count. The budget is recorded and has no
+ * effect; it stays for callers written against a later version that waits. */
 kc_status kc_ctx_set_spin_budget(kc_ctx* ctx, uint64_t ticks);
 /* The CUDA stream (a cudaStream_t) every call of this context runs on, so a
  * caller can order its own work or record timing events on it. */
