@@ -168,6 +168,8 @@ def test_golden_fixtures():
             g.orient(case.get("orientation", "degree"))
             for k, want in case["counts"].items():
                 assert g.count(int(k), "pivot") == int(want), (path.name, case["graph"], k)
+            for k, want in case.get("local", {}).items():
+                assert g.count_local(int(k)) == [int(x) for x in want], (path.name, case["graph"], k)
 
 
 def build_case(kc, spec):
