@@ -17,6 +17,12 @@
 // Unlike the reference's list kernels (|S| <= 512 or 1024 through fixed shared
 // arrays, kclique.cuh:505-516, kckernels_orientation.cuh:72-79) the lists live in
 // per-group global scratch sized from the launch's largest unit.
+//
+// The pivot traversal shares the bitmap kernel's structure: nodes with
+// r = k - held <= 2 are closed (1, |C| + drop, edges(G[C]) + drop |C| +
+// C(drop, 2)), the pivot's own branch is taken last in its parent's frame
+// (stack depth bounded by k), and a unit's tree is cut at depth 1-3 with the
+// nodes at the cut handed to the group's partitions by ticket.
 #include <algorithm>
 
 #include "count_kernels.cuh"
