@@ -15,12 +15,13 @@
 // the reference's first bucket_scan does (kclique.cuh:1610-1614, 2041).
 //
 // The persistent work queue replaces GraphQueue + bucket_scan
-// (include/GraphQueue.cuh, kclique.cuh:1318-1406): units are sorted by
-// decreasing size with a counting sort, split into size classes whose bounds
-// are computed on the device, and each class runs one persistent grid that
-// takes units from a global ticket — heavy units first, no per-window launch
-// or host synchronisation (kclique.cuh:1645-1675 launches per 1024-wide
-// degree window and syncs the host after each).
+// (include/GraphQueue.cuh, kclique.cuh:1318-1406): units are partitioned by
+// size class with a stable two-pass partition (index order, i.e. graph order,
+// inside a class), class bounds are computed on the device, and each class
+// runs one persistent grid that takes units from a global ticket; units that
+// outrun a warp's work budget go to a CTA-wide heavy pass. No per-window
+// launch or host synchronisation (kclique.cuh:1645-1675 launches per
+// 1024-wide degree window and syncs the host after each).
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -34,10 +35,26 @@ namespace kc {
 
 namespace {
 
-__global__ void k_unit_sizes(const uint32_t* __restrict__ drp, const uint32_t* __restrict__ dcol,
+struct ClassSpec {
+  int64_t lo, hi;   // unit sizes (lo, hi]
+  uint32_t G;       // threads per unit group
+  uint32_t block;   // threads per CTA
+};
+
+// Size classes, largest first.
+const ClassSpec kClasses[kNumClasses] = {
+    {1024, 0xffffffffll, 256, 256},  // CTA per unit, bitmap in global memory
+    {128, 1024, 256, 256},           // CTA per unit, bitmap in shared memory
+    {32, 128, 32, 128},              // warp per unit
+    {-1, 32, 32, 128},               // warp per unit, one word per row
+};
+__constant__ uint32_t kClassLo[kNumClasses - 1] = {1024, 128, 32};  // lower bounds of classes 0..2
+
+// Size class of every unit (kNumClasses = dropped: it cannot hold a k-clique).
+__global__ void k_unit_class(const uint32_t* __restrict__ drp, const uint32_t* __restrict__ dcol,
                              const uint32_t* __restrict__ erow, uint32_t n_units, int edge,
                              const uint32_t* __restrict__ vgraph, const uint32_t* __restrict__ gk, uint32_t k0,
-                             uint32_t* size, uint32_t* hist) {
+                             uint8_t* cls) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_units; i += gridDim.x * blockDim.x) {
     uint32_t s, src;
     if (!edge) {
@@ -53,56 +70,88 @@ __global__ void k_unit_sizes(const uint32_t* __restrict__ drp, const uint32_t* _
     if (k == 0xffffffffu || k == 0u) keep = false;  // graph not in this pass
     else if (edge) keep = k >= 2u && s >= k - 2u;
     else keep = s >= k - 1u;
-    size[i] = keep ? s : 0xffffffffu;
-    if (keep) atomicAdd(&hist[s], 1u);
+    uint8_t c = (uint8_t)kNumClasses;
+    if (keep) c = s > kClassLo[0] ? 0 : (s > kClassLo[1] ? 1 : (s > kClassLo[2] ? 2 : 3));
+    cls[i] = c;
   }
 }
 
-__global__ void k_reverse(const uint32_t* __restrict__ in, uint32_t n, uint32_t* out) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    out[i] = in[n - 1 - i];
+// Stable partition of the units by class, in two passes over chunks of
+// kPartChunk units: per-chunk class counts (class-major, so one exclusive
+// scan gives every chunk's start in every class), then an ordered scatter.
+// Units keep their index order inside a class: the units of one graph (one
+// contiguous range of rank labels) run close together and share the L2
+// lines of their out-lists.
+constexpr uint32_t kPartThreads = 256, kPartRounds = 8, kPartChunk = kPartThreads * kPartRounds;
+
+__global__ void __launch_bounds__(kPartThreads) k_class_count(const uint8_t* __restrict__ cls, uint32_t n_units,
+                                                              uint32_t n_chunks, uint32_t* cnt) {
+  __shared__ uint32_t c4[kNumClasses];
+  if (threadIdx.x < kNumClasses) c4[threadIdx.x] = 0;
+  __syncthreads();
+  const uint32_t base = blockIdx.x * kPartChunk;
+  uint32_t mine[kNumClasses] = {};
+  for (uint32_t r = 0; r < kPartRounds; ++r) {
+    const uint32_t i = base + r * kPartThreads + threadIdx.x;
+    const uint32_t c = i < n_units ? cls[i] : (uint32_t)kNumClasses;
+#pragma unroll
+    for (int q = 0; q < kNumClasses; ++q) mine[q] += c == (uint32_t)q;
+  }
+#pragma unroll
+  for (int q = 0; q < kNumClasses; ++q) {
+    uint32_t v = mine[q];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31u) == 0 && v) atomicAdd(&c4[q], v);
+  }
+  __syncthreads();
+  if (threadIdx.x < kNumClasses) cnt[(size_t)threadIdx.x * n_chunks + blockIdx.x] = c4[threadIdx.x];
 }
 
-struct ClassSpec {
-  int64_t lo, hi;   // unit sizes (lo, hi]
-  uint32_t G;       // threads per unit group
-  uint32_t block;   // threads per CTA
-};
-
-// Size classes, largest first (the queue is sorted by decreasing size).
-const ClassSpec kClasses[kNumClasses] = {
-    {1024, 0xffffffffll, 256, 256},  // CTA per unit, bitmap in global memory
-    {128, 1024, 256, 256},           // CTA per unit, bitmap in shared memory
-    {32, 128, 32, 128},              // warp per unit
-    {-1, 32, 32, 128},               // warp per unit, one word per row
-};
-
-// Class c holds the units of sizes (lo, hi], i.e. reversed indices
-// [max-hi, max-lo) of the descending order; scan = exclusive scan of the
-// reversed histogram (max + 2 entries).
-__global__ void k_class_bounds(const uint32_t* __restrict__ scan, uint32_t max_size, uint32_t* bounds) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  const int64_t M = max_size;
-  const int64_t lo[kNumClasses] = {1024, 128, 32, -1};
-  const int64_t hi[kNumClasses] = {0xffffffffll, 1024, 128, 32};
-  for (int c = 0; c < kNumClasses; ++c) {
-    uint32_t b = 0, e = 0;
-    if (M > lo[c]) {
-      const int64_t h = hi[c] < M ? hi[c] : M;
-      b = scan[M - h];
-      e = scan[M - lo[c]];
+__global__ void __launch_bounds__(kPartThreads) k_class_scatter(const uint8_t* __restrict__ cls, uint32_t n_units,
+                                                                uint32_t n_chunks, const uint32_t* __restrict__ off,
+                                                                uint32_t* queue) {
+  constexpr uint32_t kWarps = kPartThreads / 32;
+  __shared__ uint32_t wc[kWarps][kNumClasses];
+  __shared__ uint32_t run[kNumClasses];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  if (threadIdx.x < kNumClasses) run[threadIdx.x] = off[(size_t)threadIdx.x * n_chunks + blockIdx.x];
+  const uint32_t base = blockIdx.x * kPartChunk;
+  for (uint32_t r = 0; r < kPartRounds; ++r) {
+    const uint32_t i = base + r * kPartThreads + threadIdx.x;
+    const uint32_t c = i < n_units ? cls[i] : (uint32_t)kNumClasses;
+    uint32_t rank = 0;
+#pragma unroll
+    for (int q = 0; q < kNumClasses; ++q) {
+      const uint32_t m = __ballot_sync(0xffffffffu, c == (uint32_t)q);
+      if (c == (uint32_t)q) rank = __popc(m & lanemask_lt());
+      if (lane == 0) wc[warp][q] = __popc(m);
     }
+    __syncthreads();
+    if (c < (uint32_t)kNumClasses) {
+      uint32_t pos = run[c] + rank;
+      for (uint32_t w = 0; w < warp; ++w) pos += wc[w][c];
+      queue[pos] = i;
+    }
+    __syncthreads();
+    if (threadIdx.x < kNumClasses) {
+      uint32_t add = 0;
+      for (uint32_t w = 0; w < kWarps; ++w) add += wc[w][threadIdx.x];
+      run[threadIdx.x] += add;
+    }
+    __syncthreads();
+  }
+}
+
+// [begin, count] of every class from the scanned chunk counts; also stamps the
+// pass's start on the global timer (the counting kernels' time limit).
+__global__ void k_class_bounds(const uint32_t* __restrict__ off, uint32_t n_chunks, uint32_t* bounds,
+                               unsigned long long* t0) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  *t0 = global_ns();
+  for (int c = 0; c < kNumClasses; ++c) {
+    const uint32_t b = off[(size_t)c * n_chunks], e = off[(size_t)(c + 1) * n_chunks];
     bounds[2 * c] = b;
     bounds[2 * c + 1] = e - b;
-  }
-}
-
-__global__ void k_unit_scatter(const uint32_t* __restrict__ size, uint32_t n_units, uint32_t max_size,
-                               uint32_t* cursor, uint32_t* queue) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_units; i += gridDim.x * blockDim.x) {
-    const uint32_t s = size[i];
-    if (s == 0xffffffffu) continue;
-    queue[atomicAdd(&cursor[max_size - s], 1u)] = i;
   }
 }
 
@@ -132,23 +181,31 @@ kc_status ensure_binom(kc_ctx* ctx, uint32_t rows, uint32_t cols) {
     h[2 * i] = (unsigned long long)t[i];
     h[2 * i + 1] = (unsigned long long)(t[i] >> 64);
   }
+  // the new table replaces the old one only once it is complete
+  unsigned long long* nb = nullptr;
+  KC_CUDA(cudaMalloc(&nb, h.size() * sizeof(unsigned long long)));
+  const cudaError_t e = cudaMemcpy(nb, h.data(), h.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(nb);
+    return cuda_fail(e, "binomial table upload", __FILE__, __LINE__);
+  }
   cudaStreamSynchronize(ctx->stream);
   if (ctx->d_binom) cudaFree(ctx->d_binom);
-  ctx->d_binom = nullptr;
-  KC_CUDA(cudaMalloc(&ctx->d_binom, h.size() * sizeof(unsigned long long)));
-  KC_CUDA(cudaMemcpy(ctx->d_binom, h.data(), h.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+  ctx->d_binom = nb;
   ctx->brows = rows;
   ctx->bcols = cols;
   return KC_OK;
 }
 
 void count_release(CountPlan* pl) {
-  cudaStream_t s = pl->g->ctx->stream;
+  if (!pl->ctx) return;  // never prepared
+  cudaStream_t s = pl->ctx->stream;
   for (int c = 0; c <= kNumClasses; ++c) release_launch(pl->launches[c], s);
-  void* ps[] = {pl->size, pl->hist, pl->rev, pl->queue, pl->scratch, pl->heavy};
+  void* ps[] = {pl->cls, pl->ccnt, pl->queue, pl->scratch, pl->heavy};
   for (void* p : ps)
     if (p) cudaFreeAsync(p, s);
-  pl->size = pl->hist = pl->rev = pl->queue = pl->scratch = pl->heavy = nullptr;
+  pl->cls = nullptr;
+  pl->ccnt = pl->queue = pl->scratch = pl->heavy = nullptr;
 }
 
 // The context's side streams and events, created on first use.
@@ -171,9 +228,10 @@ static kc_status ensure_side(kc_ctx* ctx) {
 // enqueued (and captured) any number of times.
 kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long* d_out, uint32_t depth_boost,
                         CountPlan* pl) {
-  kc_ctx* ctx = g->ctx;
+  kc_ctx* ctx = req.ctx ? req.ctx : g->ctx;
   cudaStream_t s = ctx->stream;
   pl->g = g;
+  pl->ctx = ctx;
   pl->req = req;
   // Edge units are grouped by source when the sources' out-neighbourhoods
   // fit a shared-memory bitmap: the unit u builds G[N+(u)] once and its
@@ -192,11 +250,11 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
     return fail(KC_ERR_INVALID_ARG, "largest out-degree %u exceeds the 65534 supported per unit", pl->max_size);
   if (req.mode != KC_MODE_ORIENT) KC_TRY(ensure_binom(ctx, pl->max_size + 2, k_max + 1));
   const uint32_t nu = std::max<uint32_t>(1, pl->n_units);
-  KC_CUDA(cudaMallocAsync(&pl->size, sizeof(uint32_t) * nu, s));
+  pl->n_chunks = (nu + kPartChunk - 1) / kPartChunk;
+  KC_CUDA(cudaMallocAsync(&pl->cls, nu, s));
+  KC_CUDA(cudaMallocAsync(&pl->ccnt, sizeof(uint32_t) * ((size_t)kNumClasses * pl->n_chunks + 1), s));
   KC_CUDA(cudaMallocAsync(&pl->queue, sizeof(uint32_t) * nu, s));
   KC_CUDA(cudaMallocAsync(&pl->heavy, sizeof(uint32_t) * nu, s));
-  KC_CUDA(cudaMallocAsync(&pl->hist, sizeof(uint32_t) * ((size_t)pl->max_size + 2), s));
-  KC_CUDA(cudaMallocAsync(&pl->rev, sizeof(uint32_t) * ((size_t)pl->max_size + 2), s));
   KC_CUDA(cudaMallocAsync(&pl->scratch, sizeof(uint32_t) * kScratchWords, s));
   // Per-launch algorithm: orientation or pivot as requested; KC_MODE_AUTO
   // lists small units by orientation (cheap when their neighbourhood holds few
@@ -252,6 +310,8 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
     p.err = pl->scratch + kErrWord;
     p.stats = (req.flags & KC_FLAG_STATS) ? reinterpret_cast<unsigned long long*>(pl->scratch + kStatsWords)
                                           : nullptr;
+    p.time_limit_ns = ctx->time_limit_ns;
+    p.t0 = reinterpret_cast<const unsigned long long*>(pl->scratch + kStartWord);
     if (warp_group && budget_ok) {
       p.budget = kUnitBudget;
       p.heavy = pl->heavy;
@@ -278,18 +338,19 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
 // synchronisation, so the whole sequence can be captured in a CUDA graph.
 kc_status count_enqueue(const CountPlan& pl, cudaStream_t s) {
   kc_graph* g = pl.g;
-  const int sms = g->ctx->sms;
-  const uint32_t M = pl.max_size;
-  KC_CUDA(cudaMemsetAsync(pl.hist, 0, sizeof(uint32_t) * ((size_t)M + 2), s));
+  const int sms = pl.ctx->sms;
   KC_CUDA(cudaMemsetAsync(pl.scratch, 0, sizeof(uint32_t) * kScratchWords, s));
   const uint32_t gq = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((pl.n_units + 255) / 256, (uint64_t)sms * 16));
   if (pl.n_units)
-    k_unit_sizes<<<gq, 256, 0, s>>>(g->drp, g->dcol, g->erow, pl.n_units, pl.edge ? 1 : 0, g->vgraph,
-                                    pl.req.d_graph_k, pl.req.k, pl.size, pl.hist);
-  k_reverse<<<(M + 1 + 255) / 256, 256, 0, s>>>(pl.hist, M + 1, pl.rev);
-  KC_CUDA(prim::scan_exclusive_u32(pl.rev, pl.rev, M + 1, s));
-  k_class_bounds<<<1, 32, 0, s>>>(pl.rev, M, pl.scratch + kClassBounds);
-  if (pl.n_units) k_unit_scatter<<<gq, 256, 0, s>>>(pl.size, pl.n_units, M, pl.rev, pl.queue);
+    k_unit_class<<<gq, 256, 0, s>>>(g->drp, g->dcol, g->erow, pl.n_units, pl.edge ? 1 : 0, g->vgraph,
+                                    pl.req.d_graph_k, pl.req.k, pl.cls);
+  const uint32_t nc = pl.n_chunks;
+  if (pl.n_units) k_class_count<<<nc, kPartThreads, 0, s>>>(pl.cls, pl.n_units, nc, pl.ccnt);
+  else KC_CUDA(cudaMemsetAsync(pl.ccnt, 0, sizeof(uint32_t) * kNumClasses * (size_t)nc, s));
+  KC_CUDA(prim::scan_exclusive_u32(pl.ccnt, pl.ccnt, (size_t)kNumClasses * nc, s));
+  k_class_bounds<<<1, 32, 0, s>>>(pl.ccnt, nc, pl.scratch + kClassBounds,
+                                  reinterpret_cast<unsigned long long*>(pl.scratch + kStartWord));
+  if (pl.n_units) k_class_scatter<<<nc, kPartThreads, 0, s>>>(pl.cls, pl.n_units, nc, pl.ccnt, pl.queue);
   KC_CUDA(cudaGetLastError());
   // class launches side by side, then the heavy pass over the units they handed on
   KC_CUDA(cudaEventRecord(pl.fork, s));
@@ -310,11 +371,18 @@ kc_status count_enqueue(const CountPlan& pl, cudaStream_t s) {
   return KC_OK;
 }
 
-uint32_t count_error(const CountPlan& pl, cudaStream_t s, unsigned long long* stats3) {
+kc_status device_error_status(uint32_t err) {
+  if (err == DEV_ERR_TIMEOUT)
+    return fail(KC_ERR_DEVICE_TIMEOUT, "the counting pass ran past the context's device time limit");
+  return fail(KC_ERR_INTERNAL, "counting kernel reported device error %u", err);
+}
+
+uint32_t count_error(const CountPlan& pl, cudaStream_t s, unsigned long long* stats) {
+  static_assert(kStatsWords + 2 * kStatsCount <= kClassBounds, "stats overlap the class bounds");
   uint32_t h[kScratchWords];
   cudaMemcpyAsync(h, pl.scratch, sizeof(h), cudaMemcpyDeviceToHost, s);
   cudaStreamSynchronize(s);
-  if (stats3) std::memcpy(stats3, h + kStatsWords, 3 * sizeof(unsigned long long));
+  if (stats) std::memcpy(stats, h + kStatsWords, kStatsCount * sizeof(unsigned long long));
   return h[kErrWord];
 }
 
@@ -335,7 +403,7 @@ uint64_t count_units(const CountPlan& pl, cudaStream_t s) {
 }
 
 kc_status count_graph(kc_graph* g, const CountRequest& req, unsigned long long* d_out, kc_count_stats* stats) {
-  kc_ctx* ctx = g->ctx;
+  kc_ctx* ctx = req.ctx ? req.ctx : g->ctx;
   cudaStream_t s = ctx->stream;
   cudaEvent_t ev0, ev1;
   cudaEventCreate(&ev0);
@@ -343,7 +411,7 @@ kc_status count_graph(kc_graph* g, const CountRequest& req, unsigned long long* 
   kc_status st = KC_OK;
   uint32_t kernels = 0;
   uint64_t units = 0, heavy = 0;
-  unsigned long long sv[3] = {0, 0, 0};
+  unsigned long long sv[kStatsCount] = {};
   double ms_launch[kNumClasses + 1] = {};
   uint32_t deep = 0;
   for (uint32_t boost = 0; boost < 2; ++boost) {
@@ -378,7 +446,7 @@ kc_status count_graph(kc_graph* g, const CountRequest& req, unsigned long long* 
       KC_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long) * 2 * req.n_graphs, s));
       continue;
     }
-    if (err) st = fail(KC_ERR_INTERNAL, "counting kernel reported device error %u", err);
+    if (err) st = device_error_status(err);
     break;
   }
   if (stats && st == KC_OK) {
@@ -388,6 +456,7 @@ kc_status count_graph(kc_graph* g, const CountRequest& req, unsigned long long* 
     stats->tree_nodes = sv[0];
     stats->word_ops = sv[1];
     stats->gather_bytes = sv[2];
+    for (int q = 0; q < 3; ++q) stats->cycles[q] = sv[3 + q];
     stats->ms_total = ms;
     stats->ms_traversal = ms;
     stats->max_unit_size = g->max_out;

@@ -65,6 +65,15 @@ __device__ __forceinline__ uint32_t valid_mask(uint32_t d, uint32_t w) {  // bit
 }
 
 constexpr int kLaneStack = 16;  // lane-DFS levels: t - 2 <= 16, i.e. k <= 19 (node units)
+constexpr uint32_t kGatherRun = 8;    // warp gather: consecutive out-list words per lane per iteration
+constexpr uint32_t kSpanWords = 256;  // warp gather: membership map of up to 8192 rank labels
+
+// Offset (words) of a warp unit's gather row table inside the hash / map
+// region, which holds the hash (2 hT words) or the membership map and its
+// prefix (2 kSpanWords words).
+__host__ __device__ constexpr uint32_t gather_rows_at(uint32_t hT) {
+  return hT > kSpanWords ? 2u * hT : 2u * kSpanWords;
+}
 
 template <int NW>
 __device__ __forceinline__ void load_row(const uint32_t* B, uint32_t v, uint32_t (&r)[NW]) {
@@ -185,7 +194,7 @@ __device__ bool lane_dfs(const uint32_t* B, uint32_t d, uint32_t t, const uint32
       const uint32_t rem = t - (uint32_t)(lv + 2);
       if (rem == 1u) {
         cnt += n;
-      } else if (n >= rem) {
+      } else if (n >= rem && KC_IN_BOUNDS(lv, kLaneStack, nullptr)) {
 #pragma unroll
         for (int q = 0; q < NW; ++q) {
           stk[lv][q] = cur[q];
@@ -242,6 +251,28 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
   unsigned __int128 acc = 0;
   uint32_t acc_graph = 0xffffffffu;
   unsigned long long st_nodes = 0, st_words = 0, st_bytes = 0;
+  // With statistics, each group leader times its units' phases with the SM
+  // clock: [0] forming S and its hash, [1] gathering the induced subgraph,
+  // [2] traversing. Sums go to a per-block shared array, then to global.
+  __shared__ unsigned long long blk_cy[3];
+  const bool timing = p.stats != nullptr && gt == 0;
+  if (p.stats != nullptr) {
+    if (threadIdx.x < 3) blk_cy[threadIdx.x] = 0ull;
+    __syncthreads();
+  }
+  uint32_t tc = 0;
+  auto clk32 = []() -> uint32_t {
+    uint32_t t;
+    asm volatile("mov.u32 %0, %%clock;" : "=r"(t));
+    return t;
+  };
+  auto lap = [&](int phase) {
+    if (timing) {
+      const uint32_t t = clk32();
+      atomicAdd(&blk_cy[phase], (unsigned long long)(t - tc));  // a phase over 2^32 cycles (~2 s) wraps
+      tc = t;
+    }
+  };
 
   auto gsync = [&]() {
     if (G == 32) __syncwarp(); else __syncthreads();
@@ -287,7 +318,12 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
 
   for (;;) {
     if (gt == 0) {
-      hdr[0] = atomicAdd(p.ticket, 1u);
+      uint32_t tk = atomicAdd(p.ticket, 1u);
+      if (tk < ucnt && past_limit(p.time_limit_ns, p.t0)) {  // out of time: take no more units
+        set_error(p.err, DEV_ERR_TIMEOUT);
+        tk = 0xffffffffu;
+      }
+      hdr[0] = tk;
       hdr[1] = 0;  // subtree ticket of this unit
       hdr[4] = 0;  // nodes charged to this unit
       hdr[5] = 0;  // unit over budget
@@ -295,6 +331,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
     gsync();
     const uint32_t ui = hdr[0];
     if (ui >= ucnt) break;
+    if (timing) tc = clk32();
     const uint32_t unit = p.queue[ubeg + ui];
     uacc = 0;
     since_charge = 0;
@@ -395,7 +432,39 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
     if (LOCAL)
       for (uint32_t i = gt; i < (MODE == 0 ? d : 2u * d); i += G) loc[i] = 0ull;
     const uint32_t hshift = hT ? 33u - (uint32_t)__ffs(hT) : 0u;  // 32 - log2(hT)
-    if (hT) {
+    // A warp unit whose S spans at most kSpanWords * 32 rank labels finds
+    // local indices in a membership map of that span instead of the hash:
+    // bit x - S[0] is set for every x of S, and mpre[w] counts the members in
+    // the words below w, so x's local index (or, for a non-member, the index
+    // it would take) is mpre[w] + popc(map[w] & bits below x). Every row
+    // word lies in [S[0], ...): DAG out-lists hold only higher ranks.
+    const uint32_t s0 = S[0], last = S[d - 1];
+    const bool wmap = G == 32 && hT != 0u && last - s0 < kSpanWords * 32u;
+    uint32_t* map = hkey;
+    uint32_t* mpre = hkey + kSpanWords;
+    if (wmap) {
+      const uint32_t nmw = ((last - s0) >> 5) + 1u;
+      for (uint32_t w = lane; w < nmw; w += 32u) map[w] = 0u;
+      __syncwarp();
+      for (uint32_t i = lane; i < d; i += 32u) {
+        const uint32_t o = S[i] - s0;
+        if (KC_IN_BOUNDS(o >> 5, kSpanWords, p.err)) atomicOr(&map[o >> 5], 1u << (o & 31u));
+      }
+      __syncwarp();
+      uint32_t carry = 0;
+      for (uint32_t w0 = 0; w0 < nmw; w0 += 32u) {
+        const uint32_t w = w0 + lane;
+        const uint32_t c = w < nmw ? (uint32_t)__popc(map[w]) : 0u;
+        uint32_t incl = c;
+#pragma unroll
+        for (uint32_t o = 1; o < 32u; o <<= 1) {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += y;
+        }
+        if (w < nmw) mpre[w] = carry + incl - c;
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+      }
+    } else if (hT) {
       for (uint32_t i = gt; i < hT; i += G) hkey[i] = 0xffffffffu;
       gsync();
       for (uint32_t i = gt; i < d; i += G) {
@@ -406,32 +475,107 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
       }
     }
     gsync();
+    lap(0);
     if (G == 32 && hT) {
-      // Warp unit: one lane per row, so the 32 rows' dependent loads
-      // (row pointer, then the out-list) are in flight together; rows of a
-      // warp unit are short, and a lane's consecutive reads hit L1.
-      const uint32_t last = S[d - 1];
-      for (uint32_t j = lane; j < d; j += 32) {
-        const uint32_t x0 = S[j];
-        const uint32_t b = p.rp[x0], e = p.rp[x0 + 1];
-        uint32_t i = b;
-        for (; i < e; ++i) {
-          const uint32_t x = __ldg(p.col + i);
-          if (x > last) break;
-          uint32_t h = (x * 0x9e3779b1u) >> hshift;
-          for (uint32_t key; (key = hkey[h]) != 0xffffffffu; h = (h + 1u) & (hT - 1u)) {
-            if (key == x) {
-              const uint32_t lo = hval[h];
-              atomicOr(&B[j * Ws + (lo >> 5)], 1u << (lo & 31u));
-              if (sym) atomicOr(&B[lo * Ws + (j >> 5)], 1u << (j & 31u));
-              break;
-            }
+      // Warp unit: the out-lists of S's rows are read as one flat array,
+      // 32 kGatherRun words per iteration with every lane's loads in flight
+      // together, so the unit's whole gather costs a few memory latencies
+      // instead of one per word of its longest row. The row table (start of
+      // each row in col, exclusive prefix of the row lengths, rpre[d] = total)
+      // follows the hash / map region; word f belongs to the last row j with
+      // rpre[j] <= f.
+      uint32_t* rbase = hkey + gather_rows_at(hT);
+      uint32_t* rpre = rbase + p.dcap;
+      uint32_t carry = 0;
+      for (uint32_t j0 = 0; j0 < d; j0 += 32u) {
+        const uint32_t j = j0 + lane;
+        uint32_t b = 0, len = 0;
+        if (j < d) {
+          const uint32_t x0 = S[j];
+          b = p.rp[x0];
+          len = p.rp[x0 + 1] - b;
+        }
+        uint32_t incl = len;
+#pragma unroll
+        for (uint32_t o = 1; o < 32u; o <<= 1) {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += y;
+        }
+        if (j < d) {
+          rbase[j] = b;
+          rpre[j] = carry + incl - len;
+        }
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+      }
+      const uint32_t total = carry;
+      if (lane == 0) rpre[d] = total;
+      __syncwarp();
+      st_bytes += 4ull * (total + d);
+      // Each lane takes kGatherRun consecutive words of the flat array per
+      // iteration (lane L: words f0 + L kGatherRun ...), so one row search
+      // serves the run: its first word's row is jb (the row of the previous
+      // iteration's last word) plus the number of the next 32 row starts at or
+      // below it (a search over one start per lane), or, past 32 rows, a
+      // binary search of the rest; the later words of the run move forward
+      // over row starts one at a time. Almost every gathered word is not in S:
+      // a non-member costs one map (or hash) read, and only members pay for
+      // their local index and the bitmap atomic.
+      uint32_t jb = 0;
+      for (uint32_t f0 = 0; f0 < total; f0 += 32u * kGatherRun) {
+        const uint32_t t = jb + 1u + lane;
+        const uint32_t cand = t <= d ? rpre[t] : 0xffffffffu;
+        const uint32_t cand_last = __shfl_sync(0xffffffffu, cand, 31);
+        const uint32_t fl = f0 + lane * kGatherRun;
+        uint32_t c = 0;
+#pragma unroll
+        for (uint32_t sft = 16; sft; sft >>= 1)
+          if (__shfl_sync(0xffffffffu, cand, c + sft - 1u) <= fl) c += sft;
+        uint32_t j = jb + c;
+        if (c == 31u && cand_last <= fl) {
+          uint32_t hi = d;
+          j = jb + 32u;
+          while (hi - j > 1u) {
+            const uint32_t mid = (j + hi) >> 1;
+            if (rpre[mid] <= fl) j = mid;
+            else hi = mid;
           }
         }
-        st_bytes += 4ull * (min(i + 1u, e) - b);
+        uint32_t xs[kGatherRun], js[kGatherRun];
+#pragma unroll
+        for (uint32_t q = 0; q < kGatherRun; ++q) {
+          const uint32_t f = fl + q;
+          xs[q] = 0xffffffffu;
+          if (f < total) {
+            while (rpre[j + 1u] <= f) ++j;  // rpre[d] = total > f
+            if (KC_IN_BOUNDS(j, d, p.err)) xs[q] = __ldg(p.col + rbase[j] + (f - rpre[j]));
+          }
+          js[q] = j;
+        }
+        jb = __shfl_sync(0xffffffffu, j, 31);
+#pragma unroll
+        for (uint32_t q = 0; q < kGatherRun; ++q) {
+          const uint32_t x = xs[q];
+          if (x > last) continue;  // past every vertex of S (also the padding)
+          uint32_t lo = 0xffffffffu;
+          if (wmap) {
+            const uint32_t o = x - s0, mw = map[o >> 5];
+            if ((mw >> (o & 31u)) & 1u) lo = mpre[o >> 5] + (uint32_t)__popc(mw & ((1u << (o & 31u)) - 1u));
+          } else {
+            uint32_t h = (x * 0x9e3779b1u) >> hshift;
+            for (uint32_t hk; (hk = hkey[h]) != 0xffffffffu; h = (h + 1u) & (hT - 1u))
+              if (hk == x) {
+                lo = hval[h];
+                break;
+              }
+          }
+          if (lo == 0xffffffffu) continue;
+          const uint32_t jr = js[q];
+          if (KC_IN_BOUNDS(jr * Ws + (lo >> 5), d * Ws, p.err)) atomicOr(&B[jr * Ws + (lo >> 5)], 1u << (lo & 31u));
+          if (sym && KC_IN_BOUNDS(lo * Ws + (jr >> 5), d * Ws, p.err))
+            atomicOr(&B[lo * Ws + (jr >> 5)], 1u << (jr & 31u));
+        }
       }
     } else {
-      const uint32_t last = S[d - 1];
       for (uint32_t j = wig; j < d; j += nwg) {
         const uint32_t x0 = S[j];
         const uint32_t b = p.rp[x0], e = p.rp[x0 + 1];
@@ -456,16 +600,17 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
               }
               if (a < d && S[a] == x) lo = a;
             }
-            if (lo != 0xffffffffu) {
+            if (lo != 0xffffffffu && KC_IN_BOUNDS(lo, d, p.err)) {
               atomicOr(&B[j * Ws + (lo >> 5)], 1u << (lo & 31u));
               if (sym) atomicOr(&B[lo * Ws + (j >> 5)], 1u << (j & 31u));
             }
           }
         }
-        st_bytes += 4ull * (min(i0 + 32u, e) - b);
+        st_bytes += 4ull * (e - b + 1u);  // the row and its vertex of S (warp-uniform)
       }
     }
     gsync();
+    lap(1);
 
     if (MODE == 1 && k == (p.edge_units ? 4u : 3u)) {
       // k - hold0 = 2: the unit's count is the number of edges of G[S]; a
@@ -716,7 +861,8 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
           for (uint32_t m = nzm; m; m &= m - 1u) {
             const uint32_t q = (uint32_t)__ffs(m) - 1u;
             const uint32_t x = F[q];
-            if ((x >> pt.plane) & 1u) cand[base + __popc(x & ((1u << pt.plane) - 1u))] = q * 32u + pt.plane;
+            const uint32_t ci = base + __popc(x & ((1u << pt.plane) - 1u));
+            if (((x >> pt.plane) & 1u) && KC_IN_BOUNDS(ci, p.dcap, p.err)) cand[ci] = q * 32u + pt.plane;
             base += __popc(x);
           }
         } else {
@@ -725,7 +871,8 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
             const uint32_t x = F[q];
             if (x == 0u) continue;
             for (uint32_t b = pt.plane; b < 32u; b += pt.P)
-              if ((x >> b) & 1u) cand[base + __popc(x & ((1u << b) - 1u))] = q * 32u + b;
+              if (((x >> b) & 1u) && KC_IN_BOUNDS(base + __popc(x & ((1u << b) - 1u)), p.dcap, p.err))
+                cand[base + __popc(x & ((1u << b) - 1u))] = q * 32u + b;
             base += __popc(x);
           }
         }
@@ -965,6 +1112,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
       }
     }
     gsync();
+    lap(2);
     // commit the unit, or hand it to the heavy pass when it ran over budget
     if (budgeted && hdr[5]) {
       if (gt == 0) p.heavy[atomicAdd(p.heavy_count, 1u)] = unit;
@@ -998,7 +1146,12 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
   if (p.stats && pt.plane == 0) {
     atomicAdd(p.stats + 0, st_nodes);
     atomicAdd(p.stats + 1, st_words);
-    if (part == 0) atomicAdd(p.stats + 2, st_bytes);
+  }
+  // gather bytes are counted warp-uniformly, once per warp
+  if (p.stats && lane == 0 && st_bytes) atomicAdd(p.stats + 2, st_bytes);
+  if (p.stats != nullptr) {
+    __syncthreads();
+    if (threadIdx.x < 3) atomicAdd(p.stats + 3 + threadIdx.x, blk_cy[threadIdx.x]);
   }
 }
 
@@ -1051,14 +1204,17 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
   // counts, the drop list
   const size_t pstride = (size_t)depth * fw + (pivot ? al4(dcap) * (lp.local ? 2 : 1) : 0);
   const size_t sFr = lane ? 0 : al4((size_t)nparts * pstride);
-  const size_t limit_words = (size_t)ctx->max_smem_optin / 4;
+  const size_t limit_words = ((size_t)ctx->max_smem_optin - kStaticSmemBytes) / 4;
   // hash of S for the bitmap build: 2*hT words, hT the power of two >= 2 dcap
-  // (>= 4 dcap for warp units, whose mostly-missing lookups then probe ~1.4 slots)
+  // (load at most 1/2)
   uint32_t hT = 0;
   if (dcap <= 2048) {
     hT = 64;
-    while (hT < (G == 32 ? 4u : 2u) * dcap) hT <<= 1;
+    while (hT < 2u * dcap) hT <<= 1;
   }
+  // warp units keep their gather's row table (start and prefix of each row,
+  // 2 dcap + 1 words) behind the hash or the membership map
+  const size_t sRow = G == 32 ? al4(2 * (size_t)dcap + 1) : 0;
   bool bitmap_global = lp.force_global_bitmap;
   bool frames_global = false;
   // The hash is needed only while the bitmap is built and the frames only
@@ -1067,7 +1223,8 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
   const size_t sLoc = lp.local ? al4((pivot ? 4 : 2) * (size_t)dcap) : 0;
   auto group_words = [&]() {
     return hdr + sS + sR0 + (bitmap_global ? 0 : al4(sB)) + sLoc +
-           std::max<size_t>(frames_global ? 0 : sFr, 2 * (size_t)hT);
+           std::max<size_t>(frames_global ? 0 : sFr,
+                            !hT ? 0 : (G == 32 ? gather_rows_at(hT) + sRow : 2 * (size_t)hT));
   };
   if ((size_t)gpb * group_words() > limit_words) frames_global = true;
   if ((size_t)gpb * group_words() > limit_words) bitmap_global = true;
@@ -1100,7 +1257,14 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
                                          : (lp.local ? k_count_bitmap<1, true> : k_count_bitmap<1, false>);
   // Several classes launch the same kernel with different shared-memory sizes;
   // the attribute is per function, so it is set to the device maximum.
-  KC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->max_smem_optin));
+  // (the kernel's static shared memory counts against the same per-block limit)
+  cudaFuncAttributes fa;
+  KC_CUDA(cudaFuncGetAttributes(&fa, kern));
+  if (fa.sharedSizeBytes > kStaticSmemBytes)
+    return fail(KC_ERR_INTERNAL, "counting kernel uses %zu bytes of static shared memory, planned for %zu",
+                fa.sharedSizeBytes, kStaticSmemBytes);
+  KC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               ctx->max_smem_optin - (int)fa.sharedSizeBytes));
   int per_sm = 0;
   KC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, smem_bytes));
   per_sm = std::max(1, per_sm);

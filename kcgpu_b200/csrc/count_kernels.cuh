@@ -46,7 +46,9 @@ struct CountParams {
   size_t goff_fr;            // frames offset inside a group's global scratch
   uint32_t* ticket;          // unit ticket (zeroed)
   uint32_t* err;             // device error word
-  unsigned long long* stats; // [0] tree nodes [1] word-ops [2] gather bytes, or null
+  unsigned long long* stats; // [0] tree nodes [1] word-ops [2] gather bytes [3..5] phase cycles, or null
+  unsigned long long time_limit_ns;  // device time limit of the pass (0 = none)
+  const unsigned long long* t0;      // the pass's start on the global timer
   uint32_t budget;           // traversal nodes a unit may use before it is handed on (0 = no limit)
   uint32_t* heavy;           // units over budget, counted again by the heavy pass
   uint32_t* heavy_count;     // their number (atomic)
@@ -89,23 +91,30 @@ void release_launch(PreparedLaunch& pl, cudaStream_t s);
 constexpr int kNumClasses = 4;
 constexpr uint32_t kWarpClassMax = 128;   // largest unit a warp group takes
 constexpr uint32_t kUnitBudget = 8192;    // traversal nodes before a warp unit is handed on
+constexpr size_t kStaticSmemBytes = 64;   // static shared memory of the bitmap kernel (phase clocks), kept off the plan
 
 // Layout of a plan's scratch words (zeroed by every enqueue).
 constexpr uint32_t kScratchWords = 48;
 constexpr uint32_t kErrWord = 8;          // device error word
-constexpr uint32_t kStatsWords = 16;      // three u64 counters
+constexpr uint32_t kStatsWords = 16;      // six u64 counters: tree nodes, word-ops, gather bytes, phase cycles
+constexpr int kStatsCount = 6;
 constexpr uint32_t kClassBounds = 32;     // [begin, count] per class
 constexpr uint32_t kHeavyBounds = 40;     // [0, heavy count]
+constexpr uint32_t kStartWord = 44;       // u64: the pass's start on the global timer
 
 // Everything one counting pass needs, allocated once; enqueue may be
 // repeated and captured in a CUDA graph.
 struct CountPlan {
   kc_graph* g = nullptr;
+  kc_ctx* ctx = nullptr;    // runs the plan (the request's context, else the graph's)
   CountRequest req;
   bool edge = false;        // one unit per DAG edge
   bool edge_roots = false;  // edge units grouped by source: node units, edges as root branches
   uint32_t n_units = 0, max_size = 0;
-  uint32_t *size = nullptr, *hist = nullptr, *rev = nullptr, *queue = nullptr, *scratch = nullptr;
+  uint8_t* cls = nullptr;       // size class of every unit
+  uint32_t* ccnt = nullptr;     // per-chunk class counts, then their exclusive scan
+  uint32_t n_chunks = 0;
+  uint32_t *queue = nullptr, *scratch = nullptr;
   uint32_t* heavy = nullptr;
   unsigned long long* d_out = nullptr;
   PreparedLaunch launches[kNumClasses + 1];
@@ -124,8 +133,10 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
                         CountPlan* pl);
 kc_status count_enqueue(const CountPlan& pl, cudaStream_t s);
 void count_release(CountPlan* pl);
-// Reads the device error word (and the three stats counters when stats3 != null).
-uint32_t count_error(const CountPlan& pl, cudaStream_t s, unsigned long long* stats3);
+// Reads the device error word (and the kStatsCount stats counters when stats != null).
+uint32_t count_error(const CountPlan& pl, cudaStream_t s, unsigned long long* stats);
+// The call's status for a non-zero device error word.
+kc_status device_error_status(uint32_t err);
 uint64_t count_units(const CountPlan& pl, cudaStream_t s);
 // Units the last enqueue handed to the heavy pass.
 uint32_t count_heavy(const CountPlan& pl, cudaStream_t s);

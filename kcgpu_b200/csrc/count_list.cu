@@ -125,7 +125,12 @@ __global__ void __launch_bounds__(256) k_count_list(CountParams p, size_t cap_ed
 
   for (;;) {
     if (gt == 0) {
-      hdr[0] = atomicAdd(p.ticket, 1u);
+      uint32_t tk = atomicAdd(p.ticket, 1u);
+      if (tk < ucnt && past_limit(p.time_limit_ns, p.t0)) {  // out of time: take no more units
+        set_error(p.err, DEV_ERR_TIMEOUT);
+        tk = 0xffffffffu;
+      }
+      hdr[0] = tk;
       hdr[1] = 0;
     }
     gsync();

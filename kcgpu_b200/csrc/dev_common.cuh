@@ -14,13 +14,37 @@ enum DevErr : uint32_t {
   DEV_ERR_CAPACITY = 2,   // a unit larger than its class capacity
   DEV_ERR_TIMEOUT = 3,    // a bounded wait ran out
   DEV_ERR_INPUT = 4,      // malformed input detected on the device
+  DEV_ERR_BOUNDS = 5,     // a scratch index out of its array (KC_CHECKED builds only)
 };
 
 __device__ __forceinline__ void set_error(uint32_t* err, uint32_t code) {
   if (err) atomicCAS(err, 0u, code);
 }
 
+// KC_IN_BOUNDS(i, n, err): in a KC_CHECKED build, true when i < n and
+// otherwise records DEV_ERR_BOUNDS and returns false, so the caller skips the
+// access; in a normal build, true (no code). The checked library
+// (libkc_checked.so) stands in for the closed compute-sanitizer.
+#ifdef KC_CHECKED
+#define KC_IN_BOUNDS(i, n, err) ((uint64_t)(i) < (uint64_t)(n) ? true : (::kc::set_error((err), ::kc::DEV_ERR_BOUNDS), false))
+#else
+#define KC_IN_BOUNDS(i, n, err) true
+#endif
+
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// The GPU's global timer in nanoseconds (same epoch on every SM).
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// True when a counting pass with a device time limit has run past it; t0 is
+// the pass's start, written by the queue set-up before any counting kernel.
+__device__ __forceinline__ bool past_limit(unsigned long long limit_ns, const unsigned long long* t0) {
+  return limit_ns != 0ull && global_ns() - *(volatile const unsigned long long*)t0 > limit_ns;
+}
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
   uint32_t m;

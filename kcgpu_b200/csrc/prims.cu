@@ -259,48 +259,77 @@ __global__ void k_seg_warp(const uint32_t* __restrict__ off, uint32_t* data, uin
   }
 }
 
-// Warp per row for rows of 33..256 entries: each warp sorts its own row in a
-// private 256-word shared buffer (bitonic, __syncwarp only), so a block works
-// on eight rows at once without block-wide barriers.
-__global__ void __launch_bounds__(256) k_seg_warp_smem(const uint32_t* __restrict__ off, uint32_t* data,
-                                                       uint32_t* ucnt, const uint32_t* __restrict__ list,
-                                                       const uint32_t* count, uint32_t n_rows) {
-  __shared__ uint32_t buf[8][256];
-  const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
-  uint32_t* sm = buf[w];
+// Warp per row for rows of 33..256 entries, sorted in registers: the row is
+// padded to N = 32 E entries (E = 2, 4 or 8) and held striped, element
+// i = e * 32 + lane in register e of that lane, so loads and stores are
+// coalesced. Bitonic network: partners less than 32 apart are in other lanes
+// (one shuffle), farther partners are in another register of the same lane.
+// Dedup compares each element with its predecessor (lane - 1, or lane 31 of
+// the previous register).
+template <int E>
+__device__ __forceinline__ void warp_sort_unique_row(uint32_t* data, uint32_t b, uint32_t len, uint32_t* ucnt_r,
+                                                     uint32_t lane) {
+  uint32_t v[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const uint32_t i = (uint32_t)e * 32u + lane;
+    v[e] = i < len ? data[b + i] : 0xffffffffu;
+  }
+#pragma unroll
+  for (uint32_t k = 2; k <= 32u * E; k <<= 1) {
+#pragma unroll
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      if (j >= 32u) {
+        const uint32_t jj = j >> 5;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          if ((uint32_t)e & jj) continue;
+          const uint32_t i = (uint32_t)e * 32u + lane;
+          const uint32_t a = v[e], c = v[e ^ jj];
+          const bool asc = (i & k) == 0;
+          v[e] = asc ? min(a, c) : max(a, c);
+          v[e ^ jj] = asc ? max(a, c) : min(a, c);
+        }
+      } else {
+        const bool lower = (lane & j) == 0;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const uint32_t i = (uint32_t)e * 32u + lane;
+          const uint32_t p = __shfl_xor_sync(0xffffffffu, v[e], j);
+          const bool asc = (i & k) == 0;
+          v[e] = (lower == asc) ? min(v[e], p) : max(v[e], p);
+        }
+      }
+    }
+  }
+  uint32_t outpos = 0;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const uint32_t i = (uint32_t)e * 32u + lane;
+    const uint32_t up = __shfl_up_sync(0xffffffffu, v[e], 1);
+    const uint32_t wrap = e > 0 ? __shfl_sync(0xffffffffu, v[e > 0 ? e - 1 : 0], 31) : 0u;
+    const uint32_t prev = lane > 0 ? up : wrap;
+    const bool keep = i < len && (i == 0 || v[e] != prev);
+    const uint32_t bal = __ballot_sync(0xffffffffu, keep);
+    if (keep) data[b + outpos + __popc(bal & lanemask_lt())] = v[e];
+    outpos += __popc(bal);
+  }
+  if (lane == 0) *ucnt_r = outpos;
+}
+
+__global__ void __launch_bounds__(256) k_seg_warp_reg(const uint32_t* __restrict__ off, uint32_t* data,
+                                                      uint32_t* ucnt, const uint32_t* __restrict__ list,
+                                                      const uint32_t* count, uint32_t n_rows) {
+  const uint32_t lane = lane_id();
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
   const uint32_t cnt = min(*count, n_rows);
   for (uint32_t li = gw; li < cnt; li += nw) {
     const uint32_t r = list[li];
     const uint32_t b = off[r], len = off[r + 1] - b;
-    if (len > 256) continue;  // never index past the buffer
-    uint32_t p2 = 32;
-    while (p2 < len) p2 <<= 1;
-    for (uint32_t i = lane; i < p2; i += 32) sm[i] = i < len ? data[b + i] : 0xffffffffu;
-    __syncwarp();
-    for (uint32_t k = 2; k <= p2; k <<= 1) {
-      for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-        for (uint32_t i = lane; i < p2; i += 32) {
-          const uint32_t ixj = i ^ j;
-          if (ixj > i) {
-            const uint32_t a = sm[i], c = sm[ixj];
-            if ((a > c) == ((i & k) == 0)) { sm[i] = c; sm[ixj] = a; }
-          }
-        }
-        __syncwarp();
-      }
-    }
-    uint32_t outpos = 0;
-    for (uint32_t c0 = 0; c0 < len; c0 += 32) {
-      const uint32_t i = c0 + lane;
-      const bool keep = i < len && (i == 0 || sm[i] != sm[i - 1]);
-      const uint32_t bal = __ballot_sync(0xffffffffu, keep);
-      if (keep) data[b + outpos + __popc(bal & lanemask_lt())] = sm[i];
-      outpos += __popc(bal);
-    }
-    if (lane == 0) ucnt[r] = outpos;
-    __syncwarp();
+    if (len <= 64) warp_sort_unique_row<2>(data, b, len, ucnt + r, lane);
+    else if (len <= 128) warp_sort_unique_row<4>(data, b, len, ucnt + r, lane);
+    else if (len <= 256) warp_sort_unique_row<8>(data, b, len, ucnt + r, lane);
   }
 }
 
@@ -477,7 +506,7 @@ cudaError_t segmented_sort_unique(const uint32_t* off, uint32_t* data, uint32_t*
     k_classify_rows<<<grid, 256, 0, s>>>(off, n_rows, ucount, lists, counts, huge_total);
   }
   if (max_len > 32)
-    k_seg_warp_smem<<<sms * 8, 256, 0, s>>>(off, data, ucount, lists + (size_t)RC_W256 * n_rows, counts + RC_W256,
+    k_seg_warp_reg<<<sms * 8, 256, 0, s>>>(off, data, ucount, lists + (size_t)RC_W256 * n_rows, counts + RC_W256,
                                             n_rows);
   k_seg_warp<<<sms * 8, 256, 0, s>>>(off, data, ucount, lists + (size_t)RC_WARP * n_rows, counts + RC_WARP,
                                      n_rows);
@@ -507,13 +536,13 @@ cudaError_t segmented_sort_unique(const uint32_t* off, uint32_t* data, uint32_t*
       const uint32_t* hlist = lists + (size_t)RC_HUGE * n_rows;
       uint32_t *hlen = nullptr, *hstart = nullptr, *flag = nullptr, *pos = nullptr;
       unsigned long long *keys = nullptr, *tmp = nullptr;
-      cudaMallocAsync(&hlen, sizeof(uint32_t) * (H + 1), s);
-      cudaMallocAsync(&hstart, sizeof(uint32_t) * (H + 1), s);
-      cudaMallocAsync(&keys, sizeof(unsigned long long) * T, s);
-      cudaMallocAsync(&tmp, sizeof(unsigned long long) * T, s);
-      cudaMallocAsync(&flag, sizeof(uint32_t) * T, s);
-      cudaMallocAsync(&pos, sizeof(uint32_t) * (T + 1), s);
-      e = cudaGetLastError();
+      // every allocation is checked: a failed one must stop the sort before a kernel sees its null pointer
+      e = cudaMallocAsync(&hlen, sizeof(uint32_t) * (H + 1), s);
+      if (e == cudaSuccess) e = cudaMallocAsync(&hstart, sizeof(uint32_t) * (H + 1), s);
+      if (e == cudaSuccess) e = cudaMallocAsync(&keys, sizeof(unsigned long long) * T, s);
+      if (e == cudaSuccess) e = cudaMallocAsync(&tmp, sizeof(unsigned long long) * T, s);
+      if (e == cudaSuccess) e = cudaMallocAsync(&flag, sizeof(uint32_t) * T, s);
+      if (e == cudaSuccess) e = cudaMallocAsync(&pos, sizeof(uint32_t) * (T + 1), s);
       if (e == cudaSuccess) {
         k_huge_lengths<<<(H + 255) / 256, 256, 0, s>>>(off, hlist, H, hlen);
         e = scan_exclusive_u32(hlen, hstart, H, s);
@@ -528,12 +557,9 @@ cudaError_t segmented_sort_unique(const uint32_t* off, uint32_t* data, uint32_t*
         k_huge_count<<<(H + 255) / 256, 256, 0, s>>>(hlist, hstart, H, pos, ucount);
         if (e == cudaSuccess) e = cudaGetLastError();
       }
-      cudaFreeAsync(hlen, s);
-      cudaFreeAsync(hstart, s);
-      cudaFreeAsync(keys, s);
-      cudaFreeAsync(tmp, s);
-      cudaFreeAsync(flag, s);
-      cudaFreeAsync(pos, s);
+      void* hp[] = {hlen, hstart, keys, tmp, flag, pos};
+      for (void* p : hp)
+        if (p) cudaFreeAsync(p, s);
     }
   }
   cudaFreeAsync(lists, s);
