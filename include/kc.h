@@ -104,6 +104,10 @@ typedef struct kc_count_stats {
   uint32_t deep_retry;     /* 1 when a clique tree outgrew the fast stack and the
                               count was rerun with the full depth */
   uint32_t reserved;
+  uint64_t cycles[3];      /* SM clock cycles the unit groups spent, summed over
+                              groups: [0] forming S and its hash, [1] building the
+                              induced subgraph (gathering the out-lists),
+                              [2] the traversal */
 } kc_count_stats;
 
 typedef struct kc_graph_info {
@@ -125,18 +129,31 @@ kc_status kc_ctx_destroy(kc_ctx* ctx);
 /* Message for the last failing call on this host thread ("" if none). */
 const char* kc_last_error(void);
 const char* kc_status_string(kc_status s);
-/* Bounded-wait budget for device spin loops, in clock64 ticks (0 = default).
- * No kernel of this version spin-waits: work goes out by atomic tickets and the
- * only device-wide barrier is the cooperative-launch grid sync of the peel,
- * whose loop is bounded by the vertex count. The budget is recorded and has no
- * effect; it stays for callers written against a later version that waits. */
-kc_status kc_ctx_set_spin_budget(kc_ctx* ctx, uint64_t ticks);
+/* Device time limit of one counting pass, in nanoseconds of the GPU's global
+ * timer (0 = none, the default). The counting kernels read the timer whenever
+ * a unit group takes its next unit; once the pass has run longer than the
+ * limit they stop taking units, and the call (kc_count, kc_count_local,
+ * kc_batch_count*) returns KC_ERR_DEVICE_TIMEOUT with no count. Units already
+ * started finish, so the pass ends within one unit's time of the limit; the
+ * context stays usable. A batched call runs one pass per group of graphs that
+ * share a method, each with this limit. The reference has no counterpart (its
+ * count runs to completion, src/main.cu:303-580). */
+kc_status kc_ctx_set_time_limit(kc_ctx* ctx, uint64_t ns);
 /* The CUDA stream (a cudaStream_t) every call of this context runs on, so a
  * caller can order its own work or record timing events on it. */
 kc_status kc_ctx_get_stream(kc_ctx* ctx, void** stream);
 /* Kernels this library has launched in this process (including those
  * recorded into CUDA graphs), for accounting; monotonically increasing. */
 uint64_t kc_kernel_launches(void);
+/* Fault injection for tests, host side only (no counterpart in the reference,
+ * whose allocation failures print and continue, include/utils.cuh:44-51).
+ * kc_test_fail_alloc_after(n): the (n+1)-th device allocation the library makes
+ * from now fails as out of memory (the call returns KC_ERR_OOM); one failure,
+ * then the hook disarms; n < 0 disarms it. kc_test_live_allocations(): device
+ * allocations of the library not yet freed, to check that failing calls leak
+ * nothing. Process-wide, not per context. */
+void kc_test_fail_alloc_after(int64_t n);
+uint64_t kc_test_live_allocations(void);
 
 /* ---- graphs ---------------------------------------------------------- */
 /* Edge list in host memory (pageable or pinned). Both directions, duplicates
@@ -195,7 +212,9 @@ kc_status kc_truss_support(kc_graph* g, uint32_t* support);
  * n_nodes may be at most 262,144 (larger graphs return KC_ERR_INVALID_ARG).
  * Calls on one device share that array: calls that overlap on the GPU race and
  * must be ordered by the caller. The first call on each device looks up the
- * array's address; make it before any stream capture begins. */
+ * array's address; make it before any stream capture begins. That address
+ * lives in the device's primary context: after cudaDeviceReset the entry point
+ * must not be called again in the process. */
 kc_status kc_truss_support_noalloc(const uint32_t* d_row_ptr, const uint32_t* d_col_ind,
                                    uint32_t n_nodes, uint32_t* d_support, void* stream);
 
@@ -229,6 +248,16 @@ typedef struct kc_batch_stats {
   uint64_t word_ops;      /* with KC_FLAG_STATS: 32-bit AND+POPC word operations */
   uint64_t gather_bytes;  /* with KC_FLAG_STATS: adjacency bytes read for induced subgraphs */
   uint64_t heavy_units;   /* units handed from a warp to the CTA-wide heavy pass */
+  uint64_t cycles[3];     /* with KC_FLAG_STATS: SM cycles of the unit groups in
+                             forming S, gathering the induced subgraph, traversing */
+  double ms_csr;          /* device time of the CSR build (part of ms_build) */
+  double ms_orient;       /* device time of the orientation (part of ms_build) */
+  double host_ms[5];      /* host wall time of the call's phases: input checks and
+                             copies, build + per-graph features, method choice and
+                             plan set-up, capture + counting launch until done,
+                             read-back and release */
+  uint64_t n_vertices;    /* vertices of the batch */
+  uint64_t n_edges;       /* undirected edges after symmetrising and dedup */
 } kc_batch_stats;
 
 /* Counts every graph of the batch; counts[i] receives graph i's count and

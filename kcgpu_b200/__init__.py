@@ -65,6 +65,11 @@ class Context:
         check(lib().kc_ctx_get_stream(self._h, C.byref(s)))
         return int(s.value or 0)
 
+    def set_time_limit(self, ns: int) -> None:
+        """Device time limit of every counting pass of this context (0 = none);
+        a pass past it raises KCError KC_ERR_DEVICE_TIMEOUT."""
+        check(lib().kc_ctx_set_time_limit(self._h, int(ns)))
+
     def close(self):
         if self._h:
             lib().kc_ctx_destroy(self._h)
@@ -198,6 +203,7 @@ class Graph:
         if stats:
             vals = {f: getattr(st, f) for f, _ in KcCountStats._fields_ if f != "reserved"}
             vals["ms_launch"] = list(vals["ms_launch"])
+            vals["cycles"] = list(vals["cycles"])
             return CountResult(out.value(), vals)
         return out.value()
 
@@ -316,17 +322,18 @@ class SingleGPU_Kclique_Local:
 # ---- synthetic inputs ---------------------------------------------------------
 
 class EdgeList:
-    """A host edge list owned by the library (optionally page-locked)."""
+    """A host edge list owned by the library that made it (optionally page-locked)."""
 
-    def __init__(self, handle):
+    def __init__(self, handle, library=None):
         self._h = handle
+        self._L = library if library is not None else lib()
 
     def arrays(self, copy: bool = True):
         s = C.POINTER(C.c_uint32)()
         d = C.POINTER(C.c_uint32)()
         ne = C.c_uint64()
         nn = C.c_uint32()
-        check(lib().kc_edgelist_data(self._h, C.byref(s), C.byref(d), C.byref(ne), C.byref(nn)))
+        check(self._L.kc_edgelist_data(self._h, C.byref(s), C.byref(d), C.byref(ne), C.byref(nn)))
         n = int(ne.value)
         if n == 0:
             return np.zeros(0, np.uint32), np.zeros(0, np.uint32), int(nn.value)
@@ -341,11 +348,11 @@ class EdgeList:
         d = C.POINTER(C.c_uint32)()
         ne = C.c_uint64()
         nn = C.c_uint32()
-        check(lib().kc_edgelist_data(self._h, C.byref(s), C.byref(d), C.byref(ne), C.byref(nn)))
+        check(self._L.kc_edgelist_data(self._h, C.byref(s), C.byref(d), C.byref(ne), C.byref(nn)))
         return s, d, int(ne.value), int(nn.value)
 
     def plant_cliques(self, count: int, smin: int, smax: int, seed: int):
-        check(lib().kc_gen_plant_cliques(self._h, count, smin, smax, seed))
+        check(self._L.kc_gen_plant_cliques(self._h, count, smin, smax, seed))
         return self
 
     def batch_meta(self):
@@ -354,14 +361,14 @@ class EdgeList:
         kk = C.POINTER(C.c_uint32)()
         fam = C.POINTER(C.c_uint32)()
         ng = C.c_uint32()
-        check(lib().kc_batchgen_meta(self._h, C.byref(off), C.byref(nn), C.byref(kk), C.byref(fam), C.byref(ng)))
+        check(self._L.kc_batchgen_meta(self._h, C.byref(off), C.byref(nn), C.byref(kk), C.byref(fam), C.byref(ng)))
         g = int(ng.value)
         return (np.ctypeslib.as_array(off, shape=(g + 1,)).copy(), np.ctypeslib.as_array(nn, shape=(g,)).copy(),
                 np.ctypeslib.as_array(kk, shape=(g,)).copy(), np.ctypeslib.as_array(fam, shape=(g,)).copy())
 
     def close(self):
         if self._h:
-            lib().kc_edgelist_destroy(self._h)
+            self._L.kc_edgelist_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -371,10 +378,21 @@ class EdgeList:
             pass
 
 
-def _gen(fn, *args) -> EdgeList:
+def _gen(fn, *args, library=None) -> EdgeList:
     h = C.c_void_p()
-    check(fn(*args, C.byref(h)))
-    return EdgeList(h)
+    st = fn(*args, C.byref(h))
+    if st != 0:
+        L = library if library is not None else lib()
+        raise KCError(st, L.kc_last_error().decode(errors="replace"))
+    return EdgeList(h, library)
+
+
+def gen_batch_host(n_graphs: int, base_seed: int, n_min=50, n_max=5000, k_min=4, k_max=12) -> EdgeList:
+    """gen_batch through the generator-only library (libkcgen.so): the same
+    seeded batch in pageable host memory, for a process that must not load
+    the engine."""
+    G = _lib.load_gen()
+    return _gen(G.kc_gen_batch, n_graphs, base_seed, n_min, n_max, k_min, k_max, 0, library=G)
 
 
 def read_edgelist(path, format: str = "auto", pinned: bool = False) -> EdgeList:
@@ -447,7 +465,10 @@ def batch_count(ctx: Context, src, dst, edge_off, n_nodes, ks, orientation="degr
         out.append([{"mode": int(c.mode), "unit": int(c.unit), "part": int(c.part), "encoding": int(c.encoding)}
                     for c in choice])
     if return_stats:
-        out.append({f: getattr(st, f) for f, _ in KcBatchStats._fields_})
+        vals = {f: getattr(st, f) for f, _ in KcBatchStats._fields_}
+        vals["cycles"] = list(vals["cycles"])
+        vals["host_ms"] = list(vals["host_ms"])
+        out.append(vals)
     return out[0] if len(out) == 1 else tuple(out)
 
 

@@ -6,6 +6,7 @@ import fails loudly (there is no CPU fallback for any engine call).
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 _LIB_PATH = Path(__file__).resolve().parent / "libkc.so"
@@ -29,7 +30,7 @@ class KcCountStats(C.Structure):
     _fields_ = [("units", u64), ("tree_nodes", u64), ("word_ops", u64), ("gather_bytes", u64),
                 ("ms_total", C.c_double), ("ms_traversal", C.c_double), ("max_unit_size", u32),
                 ("kernels", u32), ("ms_launch", C.c_double * 5), ("heavy_units", u64), ("deep_retry", u32),
-                ("reserved", u32)]
+                ("reserved", u32), ("cycles", u64 * 3)]
 
 
 class KcGraphInfo(C.Structure):
@@ -49,7 +50,9 @@ class KcBatchOpts(C.Structure):
 class KcBatchStats(C.Structure):
     _fields_ = [("ms_total", C.c_double), ("ms_h2d", C.c_double), ("ms_build", C.c_double),
                 ("ms_count", C.c_double), ("units", u64), ("kernels", u32), ("n_graphs", u32),
-                ("tree_nodes", u64), ("word_ops", u64), ("gather_bytes", u64), ("heavy_units", u64)]
+                ("tree_nodes", u64), ("word_ops", u64), ("gather_bytes", u64), ("heavy_units", u64),
+                ("cycles", u64 * 3), ("ms_csr", C.c_double), ("ms_orient", C.c_double),
+                ("host_ms", C.c_double * 5), ("n_vertices", u64), ("n_edges", u64)]
 
 
 class KcServerOpts(C.Structure):
@@ -68,9 +71,11 @@ SIGNATURES = {
     "kc_ctx_destroy": (i32, [C.c_void_p]),
     "kc_last_error": (C.c_char_p, []),
     "kc_status_string": (C.c_char_p, [i32]),
-    "kc_ctx_set_spin_budget": (i32, [C.c_void_p, u64]),
+    "kc_ctx_set_time_limit": (i32, [C.c_void_p, u64]),
     "kc_ctx_get_stream": (i32, [C.c_void_p, P(C.c_void_p)]),
     "kc_kernel_launches": (u64, []),
+    "kc_test_fail_alloc_after": (None, [i64]),
+    "kc_test_live_allocations": (u64, []),
     "kc_graph_from_edges": (i32, [C.c_void_p, P(u32), P(u32), u64, u32, P(C.c_void_p)]),
     "kc_graph_from_edges_device": (i32, [C.c_void_p, C.c_void_p, C.c_void_p, u64, u32, P(C.c_void_p)]),
     "kc_graph_from_csr": (i32, [C.c_void_p, P(u32), P(u32), u32, P(C.c_void_p)]),
@@ -135,7 +140,10 @@ def load(path: Path | None = None) -> C.CDLL:
     global _lib
     if _lib is not None:
         return _lib
-    p = Path(path) if path else _LIB_PATH
+    # KC_LIBRARY names another build of the engine in this package (tests load
+    # the bounds-checked libkc_checked.so that way)
+    alt = os.environ.get("KC_LIBRARY")
+    p = Path(path) if path else (_LIB_PATH.parent / alt if alt else _LIB_PATH)
     if not p.exists():
         raise ImportError(f"{p} is missing: build it with `python -m kcgpu_b200.build` (nvcc, sm_100a)")
     lib = C.CDLL(str(p))
@@ -145,6 +153,26 @@ def load(path: Path | None = None) -> C.CDLL:
         f.argtypes = args
     _lib = lib
     return lib
+
+
+_gen_lib = None
+_GEN_PATH = Path(__file__).resolve().parent / "libkcgen.so"
+_GEN_SIGNATURES = ("kc_last_error", "kc_edgelist_data", "kc_edgelist_destroy", "kc_gen_er", "kc_gen_rmat",
+                   "kc_gen_chung_lu", "kc_gen_sbm", "kc_gen_plant_cliques", "kc_gen_batch", "kc_batchgen_meta")
+
+
+def load_gen() -> C.CDLL:
+    """Loads libkcgen.so (the seeded generators without the engine) once."""
+    global _gen_lib
+    if _gen_lib is None:
+        if not _GEN_PATH.exists():
+            raise ImportError(f"{_GEN_PATH} is missing: build it with `python -m kcgpu_b200.build`")
+        g = C.CDLL(str(_GEN_PATH))
+        for name in _GEN_SIGNATURES:
+            f = getattr(g, name)
+            f.restype, f.argtypes = SIGNATURES[name]
+        _gen_lib = g
+    return _gen_lib
 
 
 def check(status: int) -> None:

@@ -77,9 +77,11 @@ uint32_t grid_for(uint64_t work, int sms) {
 }
 
 void free_union(kc_graph* g) {
-  void* ps[] = {g->rp, g->col, g->rank, g->inv, g->drp, g->dcol, g->erow, g->prio, g->level, g->vgraph};
-  for (void* p : ps)
-    if (p) cudaFreeAsync(p, g->ctx->stream);
+  uint32_t** ps[] = {&g->rp, &g->col, &g->rank, &g->inv, &g->drp, &g->dcol, &g->erow, &g->prio, &g->level, &g->vgraph};
+  for (uint32_t** p : ps) {
+    if (*p) cudaFreeAsync(*p, g->ctx->stream);
+    *p = nullptr;
+  }
 }
 
 struct Choice {
@@ -111,16 +113,40 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool 
   const uint64_t E = edge_off[G] - edge_off[0];
   const uint32_t orientation = opts ? opts->orientation : KC_ORIENT_DEGREE;
 
-  cudaEvent_t e0, e1, e2, e3, e4;
+  // Everything the call creates is released on every return path: device
+  // temporaries by t, the union graph, plans, captured graph and events by
+  // the guard below.
+  cudaEvent_t e0, e1, e2, e3, e4, ec, eo;  // ec / eo: CSR built / orientation done
   cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2); cudaEventCreate(&e3); cudaEventCreate(&e4);
+  cudaEventCreate(&ec); cudaEventCreate(&eo);
+  kc_graph U;
+  U.ctx = ctx;
+  std::vector<CountPlan> plans;
+  cudaGraph_t cg = nullptr;
+  cudaGraphExec_t cge = nullptr;
+  DevTemps t(s);
+  struct Release {
+    kc_graph* U;
+    std::vector<CountPlan>* plans;
+    cudaGraph_t* cg;
+    cudaGraphExec_t* cge;
+    cudaEvent_t ev[7];
+    ~Release() {
+      if (*cge) cudaGraphExecDestroy(*cge);
+      if (*cg) cudaGraphDestroy(*cg);
+      for (auto& pl : *plans) count_release(&pl);
+      free_union(U);
+      for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    }
+  } release{&U, &plans, &cg, &cge, {e0, e1, e2, e3, e4, ec, eo}};
   uint32_t *ds = nullptr, *dd = nullptr, *dvoff = nullptr, *dnn = nullptr, *derr = nullptr, *vg = nullptr;
   unsigned long long* deoff = nullptr;
-  KC_CUDA(cudaMallocAsync(&ds, sizeof(uint32_t) * std::max<uint64_t>(1, E), s));
-  KC_CUDA(cudaMallocAsync(&dd, sizeof(uint32_t) * std::max<uint64_t>(1, E), s));
-  KC_CUDA(cudaMallocAsync(&deoff, sizeof(unsigned long long) * ((size_t)G + 1), s));
-  KC_CUDA(cudaMallocAsync(&dvoff, sizeof(uint32_t) * ((size_t)G + 1), s));
-  KC_CUDA(cudaMallocAsync(&dnn, sizeof(uint32_t) * G, s));
-  KC_CUDA(cudaMallocAsync(&derr, sizeof(uint32_t) * 4, s));
+  KC_CUDA(t.alloc(&ds, sizeof(uint32_t) * std::max<uint64_t>(1, E)));
+  KC_CUDA(t.alloc(&dd, sizeof(uint32_t) * std::max<uint64_t>(1, E)));
+  KC_CUDA(t.alloc(&deoff, sizeof(unsigned long long) * ((size_t)G + 1)));
+  KC_CUDA(t.alloc(&dvoff, sizeof(uint32_t) * ((size_t)G + 1)));
+  KC_CUDA(t.alloc(&dnn, sizeof(uint32_t) * G));
+  KC_CUDA(t.alloc(&derr, sizeof(uint32_t) * 4));
   KC_CUDA(cudaMemsetAsync(derr, 0, sizeof(uint32_t) * 4, s));
   std::vector<unsigned long long> eoff_rel((size_t)G + 1);
   for (uint32_t g = 0; g <= G; ++g) eoff_rel[g] = edge_off[g] - edge_off[0];
@@ -140,18 +166,20 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool 
   KC_CUDA(cudaStreamSynchronize(s));
   if (herr) return fail(KC_ERR_INVALID_ARG, "graph %u has an endpoint not below its n_nodes", herr - 1);
 
-  kc_graph U;
-  U.ctx = ctx;
+  double th[6] = {t0, 0, 0, 0, 0, 0};  // host phase boundaries (stats->host_ms)
+  th[1] = now_ms();
   kc_status st = build_csr(&U, ds, dd, E, (uint32_t)N);
-  cudaFreeAsync(ds, s);
-  cudaFreeAsync(dd, s);
+  cudaEventRecord(ec, s);
+  t.free_now(ds);
+  t.free_now(dd);
   // graph of every original vertex: gives each graph a contiguous rank range
   if (st == KC_OK) {
-    KC_CUDA(cudaMallocAsync(&vg, sizeof(uint32_t) * std::max<uint64_t>(1, N), s));
+    KC_CUDA(t.alloc(&vg, sizeof(uint32_t) * std::max<uint64_t>(1, N)));
     k_vertex_graph<<<std::min<uint32_t>(G, 65535), 256, 0, s>>>(dvoff, G, vg);
     U.vgraph_orig = vg;
     U.n_graphs = G;
     st = orient_graph(&U, orientation);
+    cudaEventRecord(eo, s);
     U.vgraph_orig = nullptr;
   }
   if (st == KC_OK) st = dev_alloc(&U, (void**)&U.vgraph, sizeof(uint32_t) * std::max<uint64_t>(1, N));
@@ -161,9 +189,9 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool 
     k_rank_graph<<<grid_for(N, ctx->sms), 256, 0, s>>>(vg, U.rank, (uint32_t)N, U.vgraph);
     uint32_t *dfmax = nullptr, *dfcore = nullptr;
     unsigned long long* dfm = nullptr;
-    KC_CUDA(cudaMallocAsync(&dfmax, sizeof(uint32_t) * G, s));
-    KC_CUDA(cudaMallocAsync(&dfcore, sizeof(uint32_t) * G, s));
-    KC_CUDA(cudaMallocAsync(&dfm, sizeof(unsigned long long) * G, s));
+    KC_CUDA(t.alloc(&dfmax, sizeof(uint32_t) * G));
+    KC_CUDA(t.alloc(&dfcore, sizeof(uint32_t) * G));
+    KC_CUDA(t.alloc(&dfm, sizeof(unsigned long long) * G));
     KC_CUDA(cudaMemsetAsync(dfmax, 0, sizeof(uint32_t) * G, s));
     KC_CUDA(cudaMemsetAsync(dfcore, 0, sizeof(uint32_t) * G, s));
     KC_CUDA(cudaMemsetAsync(dfm, 0, sizeof(unsigned long long) * G, s));
@@ -174,12 +202,13 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool 
     KC_CUDA(cudaMemcpyAsync(fm.data(), dfm, sizeof(unsigned long long) * G, cudaMemcpyDeviceToHost, s));
     cudaEventRecord(e2, s);
     KC_CUDA(cudaStreamSynchronize(s));
-    cudaFreeAsync(dfmax, s);
-    cudaFreeAsync(dfcore, s);
-    cudaFreeAsync(dfm, s);
+    t.free_now(dfmax);
+    t.free_now(dfcore);
+    t.free_now(dfm);
   }
-  if (vg) cudaFreeAsync(vg, s);
+  if (vg) t.free_now(vg);
 
+  th[2] = now_ms();
   // per-graph choices, grouped into counting passes
   std::map<Choice, std::vector<uint32_t>> groups;
   std::vector<kc_params> picked(G);
@@ -205,14 +234,10 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool 
   }
 
   unsigned long long* dout = nullptr;
-  std::vector<uint32_t*> gks;
-  std::vector<CountPlan> plans;
-  cudaGraph_t cg = nullptr;
-  cudaGraphExec_t cge = nullptr;
   uint32_t kernels = 0;
   uint64_t units = 0;
   if (st == KC_OK) {
-    KC_CUDA(cudaMallocAsync(&dout, sizeof(unsigned long long) * 2 * G, s));
+    KC_CUDA(t.alloc(&dout, sizeof(unsigned long long) * 2 * G));
     plans.reserve(groups.size());
     for (auto& kv : groups) {
       std::vector<uint32_t> hk(G, 0xffffffffu);
@@ -222,9 +247,8 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool 
         kmax = std::max(kmax, ks[g]);
       }
       uint32_t* dk = nullptr;
-      KC_CUDA(cudaMallocAsync(&dk, sizeof(uint32_t) * G, s));
+      KC_CUDA(t.alloc(&dk, sizeof(uint32_t) * G));
       KC_CUDA(cudaMemcpyAsync(dk, hk.data(), sizeof(uint32_t) * G, cudaMemcpyHostToDevice, s));
-      gks.push_back(dk);
       CountRequest req;
       req.k = kmax;
       req.mode = kv.first.mode;
@@ -243,6 +267,7 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool 
   if (st == KC_OK) {
     KC_CUDA(cudaMemsetAsync(dout, 0, sizeof(unsigned long long) * 2 * G, s));
     KC_CUDA(cudaStreamSynchronize(s));
+    th[3] = now_ms();
     const bool use_graph = !opts || opts->use_graph;
     if (use_graph) {
       KC_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -271,16 +296,16 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool 
       cudaEventRecord(e4, s);
     }
   }
-  unsigned long long trav[3] = {0, 0, 0};
+  unsigned long long trav[kStatsCount] = {};
   uint64_t heavy_units = 0;
   if (st == KC_OK) {
     bool deep = false;
     for (auto& pl : plans) {
-      unsigned long long sv[3] = {0, 0, 0};
+      unsigned long long sv[kStatsCount] = {};
       uint32_t err = count_error(pl, s, sv);
       if (err == DEV_ERR_STACK) deep = true;
-      else if (err) st = fail(KC_ERR_INTERNAL, "batched counting reported device error %u", err);
-      for (int q = 0; q < 3; ++q) trav[q] += sv[q];
+      else if (err && st == KC_OK) st = device_error_status(err);
+      for (int q = 0; q < kStatsCount; ++q) trav[q] += sv[q];
       heavy_units += count_heavy(pl, s);
       units += count_units(pl, s);
       kernels += 5;
@@ -297,11 +322,12 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool 
         if (st == KC_OK) st = count_enqueue(plans[i], s);
         if (st == KC_OK) {
           uint32_t err = count_error(plans[i], s, nullptr);
-          if (err) st = fail(KC_ERR_INTERNAL, "batched counting reported device error %u", err);
+          if (err) st = device_error_status(err);
         }
       }
     }
   }
+  th[4] = now_ms();
   std::vector<unsigned long long> hout(2 * (size_t)G, 0);
   if (st == KC_OK) {
     KC_CUDA(cudaMemcpyAsync(hout.data(), dout, sizeof(unsigned long long) * 2 * G, cudaMemcpyDeviceToHost, s));
@@ -312,8 +338,8 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool 
       if (choice) choice[g] = picked[g];
     }
   }
-  if (stats) {
-    std::memset(stats, 0, sizeof(*stats));
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  if (stats && st == KC_OK) {  // (a failed call may not have recorded the events)
     float a = 0, b = 0, c = 0;
     cudaEventElapsedTime(&a, e0, e1);
     cudaEventElapsedTime(&b, e1, e2);
@@ -321,6 +347,10 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool 
     stats->ms_h2d = a;
     stats->ms_build = b;
     stats->ms_count = c;
+    cudaEventElapsedTime(&a, e1, ec);
+    stats->ms_csr = a;
+    cudaEventElapsedTime(&a, ec, eo);
+    stats->ms_orient = a;
     stats->units = units;
     stats->kernels = kernels;
     stats->n_graphs = G;
@@ -328,20 +358,16 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool 
     stats->word_ops = trav[1];
     stats->gather_bytes = trav[2];
     stats->heavy_units = heavy_units;
+    for (int q = 0; q < 3; ++q) stats->cycles[q] = trav[3 + q];
   }
-  if (cge) cudaGraphExecDestroy(cge);
-  if (cg) cudaGraphDestroy(cg);
-  for (auto& pl : plans) count_release(&pl);
-  for (auto* p : gks) cudaFreeAsync(p, s);
-  if (dout) cudaFreeAsync(dout, s);
-  cudaFreeAsync(deoff, s);
-  cudaFreeAsync(dvoff, s);
-  cudaFreeAsync(dnn, s);
-  cudaFreeAsync(derr, s);
-  free_union(&U);
   cudaStreamSynchronize(s);
-  cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2); cudaEventDestroy(e3); cudaEventDestroy(e4);
-  if (stats) stats->ms_total = now_ms() - t0;
+  th[5] = now_ms();
+  if (stats) {
+    stats->ms_total = th[5] - t0;
+    for (int q = 0; q < 5; ++q) stats->host_ms[q] = th[q + 1] > 0 && th[q] > 0 ? th[q + 1] - th[q] : 0.0;
+    stats->n_vertices = N;
+    stats->n_edges = U.m;
+  }
   return st;
 }
 

@@ -68,8 +68,9 @@ kc_status build_csr(kc_graph* g, const uint32_t* d_src, const uint32_t* d_dst, u
   const int sms = g->ctx->sms;
   const uint32_t grid_e = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((E + 255) / 256, (uint64_t)sms * 16));
 
+  DevTemps tmp(s);
   uint32_t* scal = nullptr;  // [0] max id, [1] max row length (with duplicates), [2] max degree
-  KC_CUDA(cudaMallocAsync(&scal, 4 * sizeof(uint32_t), s));
+  KC_CUDA(tmp.alloc(&scal, 4 * sizeof(uint32_t)));
   KC_CUDA(cudaMemsetAsync(scal, 0, 4 * sizeof(uint32_t), s));
   uint32_t h[4] = {0, 0, 0, 0};
   if (E) {
@@ -80,21 +81,18 @@ kc_status build_csr(kc_graph* g, const uint32_t* d_src, const uint32_t* d_dst, u
   }
   uint32_t n = n_nodes;
   if (n == 0) {
-    if (E && h[0] == 0xffffffffu) { cudaFreeAsync(scal, s); return fail(KC_ERR_INVALID_ARG, "vertex id 0xffffffff is reserved"); }
+    if (E && h[0] == 0xffffffffu) return fail(KC_ERR_INVALID_ARG, "vertex id 0xffffffff is reserved");
     n = E ? h[0] + 1 : 0;
   } else if (E && h[0] >= n) {
-    cudaFreeAsync(scal, s);
     return fail(KC_ERR_INVALID_ARG, "edge endpoint %u is not below n_nodes = %u", h[0], n);
   }
-  if (2 * E >= 0xffffffffull) {
-    cudaFreeAsync(scal, s);
+  if (2 * E >= 0xffffffffull)
     return fail(KC_ERR_INVALID_ARG, "%llu input edges exceed the 32-bit offset range", (unsigned long long)E);
-  }
   g->n = n;
 
   uint32_t *deg = nullptr, *off = nullptr, *adj = nullptr, *ucnt = nullptr;
-  KC_CUDA(cudaMallocAsync(&deg, sizeof(uint32_t) * ((size_t)n + 1), s));
-  KC_CUDA(cudaMallocAsync(&off, sizeof(uint32_t) * ((size_t)n + 1), s));
+  KC_CUDA(tmp.alloc(&deg, sizeof(uint32_t) * ((size_t)n + 1)));
+  KC_CUDA(tmp.alloc(&off, sizeof(uint32_t) * ((size_t)n + 1)));
   KC_CUDA(cudaMemsetAsync(deg, 0, sizeof(uint32_t) * ((size_t)n + 1), s));
   if (E) k_degree<<<grid_e, 256, 0, s>>>(d_src, d_dst, E, deg);
   KC_CUDA(prim::scan_exclusive_u32(deg, off, n, s));
@@ -104,13 +102,13 @@ kc_status build_csr(kc_graph* g, const uint32_t* d_src, const uint32_t* d_dst, u
   KC_CUDA(cudaMemcpyAsync(h + 1, scal + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   KC_CUDA(cudaStreamSynchronize(s));
 
-  KC_CUDA(cudaMallocAsync(&adj, sizeof(uint32_t) * std::max<size_t>(1, total), s));
+  KC_CUDA(tmp.alloc(&adj, sizeof(uint32_t) * std::max<size_t>(1, total)));
   // deg is reused as the scatter cursor (a copy of the offsets)
   KC_CUDA(cudaMemcpyAsync(deg, off, sizeof(uint32_t) * ((size_t)n + 1), cudaMemcpyDeviceToDevice, s));
   if (E) k_scatter<<<grid_e, 256, 0, s>>>(d_src, d_dst, E, deg, adj);
   KC_CUDA(cudaGetLastError());
 
-  KC_CUDA(cudaMallocAsync(&ucnt, sizeof(uint32_t) * ((size_t)n + 1), s));
+  KC_CUDA(tmp.alloc(&ucnt, sizeof(uint32_t) * ((size_t)n + 1)));
   KC_CUDA(prim::segmented_sort_unique(off, adj, ucnt, n, h[1], s));
 
   // final offsets and compaction into the graph's own arrays
@@ -125,12 +123,6 @@ kc_status build_csr(kc_graph* g, const uint32_t* d_src, const uint32_t* d_dst, u
   KC_CUDA(prim::compact_rows(off, adj, g->rp, g->col, n, s));
   g->m = m2 / 2;
   g->max_deg = h[2];
-
-  cudaFreeAsync(deg, s);
-  cudaFreeAsync(off, s);
-  cudaFreeAsync(adj, s);
-  cudaFreeAsync(ucnt, s);
-  cudaFreeAsync(scal, s);
   KC_CUDA(cudaGetLastError());
   return KC_OK;
 }

@@ -21,30 +21,6 @@
 
 namespace kc {
 
-namespace {
-thread_local std::string g_last_error;
-}
-
-kc_status fail(kc_status st, const char* fmt, ...) {
-  char buf[1024];
-  va_list ap;
-  va_start(ap, fmt);
-  vsnprintf(buf, sizeof(buf), fmt, ap);
-  va_end(ap);
-  g_last_error = buf;
-  return st;
-}
-
-void clear_error() { g_last_error.clear(); }
-
-kc_status cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
-  cudaGetLastError();
-  const char* base = std::strrchr(file, '/');
-  base = base ? base + 1 : file;
-  kc_status st = (e == cudaErrorMemoryAllocation) ? KC_ERR_OOM : KC_ERR_CUDA;
-  return fail(st, "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), base, line);
-}
-
 kc_status dev_alloc(kc_graph* g, void** p, size_t bytes) {
   bytes = std::max<size_t>(bytes, 4);
   cudaError_t e = cudaMallocAsync(p, bytes, g->ctx->stream);
@@ -153,23 +129,6 @@ cudaError_t __wrap_cudaLaunchCooperativeKernel(const void* f, dim3 g, dim3 b, vo
 
 uint64_t kc_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
 
-const char* kc_last_error(void) { return kc::g_last_error.c_str(); }
-
-const char* kc_status_string(kc_status s) {
-  switch (s) {
-    case KC_OK: return "ok";
-    case KC_ERR_INVALID_ARG: return "invalid argument";
-    case KC_ERR_OOM: return "out of memory";
-    case KC_ERR_ADMISSION: return "admission rejected";
-    case KC_ERR_DEVICE_TIMEOUT: return "device wait timed out";
-    case KC_ERR_CUDA: return "CUDA error";
-    case KC_ERR_INTERNAL: return "internal error";
-    case KC_ERR_NOT_ORIENTED: return "graph not oriented";
-    case KC_ERR_CANCELLED: return "cancelled";
-    case KC_ERR_BUSY: return "busy";
-  }
-  return "unknown status";
-}
 
 kc_status kc_ctx_create(int device, kc_ctx** out) {
   kc::clear_error();
@@ -225,9 +184,10 @@ kc_status kc_ctx_destroy(kc_ctx* ctx) {
   return KC_OK;
 }
 
-kc_status kc_ctx_set_spin_budget(kc_ctx* ctx, uint64_t ticks) {
+kc_status kc_ctx_set_time_limit(kc_ctx* ctx, uint64_t ns) {
   if (!ctx) return fail(KC_ERR_INVALID_ARG, "context is NULL");
-  ctx->spin_budget = ticks;
+  std::lock_guard<std::mutex> l(ctx->mu);
+  ctx->time_limit_ns = ns;
   return KC_OK;
 }
 
@@ -245,20 +205,18 @@ kc_status kc_graph_from_edges(kc_ctx* ctx, const uint32_t* src, const uint32_t* 
   kc_graph* g;
   KC_TRY(kc::new_graph(ctx, &g));
   cudaStream_t s = ctx->stream;
-  uint32_t *ds = nullptr, *dd = nullptr;
-  size_t bytes = std::max<uint64_t>(1, n_edges) * sizeof(uint32_t);
-  cudaError_t e1 = cudaMallocAsync(&ds, bytes, s), e2 = cudaMallocAsync(&dd, bytes, s);
-  if (e1 != cudaSuccess || e2 != cudaSuccess) {
-    delete g;
-    return kc::cuda_fail(e1 != cudaSuccess ? e1 : e2, "edge staging allocation", __FILE__, __LINE__);
+  kc_status st = KC_OK;
+  {
+    kc::DevTemps t(s);
+    uint32_t *ds = nullptr, *dd = nullptr;
+    const size_t bytes = std::max<uint64_t>(1, n_edges) * sizeof(uint32_t);
+    cudaError_t e = t.alloc(&ds, bytes);
+    if (e == cudaSuccess) e = t.alloc(&dd, bytes);
+    if (e == cudaSuccess && n_edges) e = cudaMemcpyAsync(ds, src, n_edges * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && n_edges) e = cudaMemcpyAsync(dd, dst, n_edges * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+    st = e == cudaSuccess ? kc::build_from_device(g, ds, dd, n_edges, n_nodes)
+                          : kc::cuda_fail(e, "edge staging", __FILE__, __LINE__);
   }
-  if (n_edges) {
-    cudaMemcpyAsync(ds, src, n_edges * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(dd, dst, n_edges * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
-  }
-  kc_status st = kc::build_from_device(g, ds, dd, n_edges, n_nodes);
-  cudaFreeAsync(ds, s);
-  cudaFreeAsync(dd, s);
   if (st != KC_OK) {
     kc::free_graph_arrays(g);
     delete g;
@@ -297,19 +255,22 @@ kc_status kc_graph_from_csr(kc_ctx* ctx, const uint32_t* row_ptr, const uint32_t
   kc_graph* g;
   KC_TRY(kc::new_graph(ctx, &g));
   cudaStream_t s = ctx->stream;
-  uint32_t *drp = nullptr, *ds = nullptr, *dd = nullptr;
-  KC_CUDA(cudaMallocAsync(&drp, sizeof(uint32_t) * ((size_t)n_nodes + 1), s));
-  KC_CUDA(cudaMallocAsync(&ds, sizeof(uint32_t) * std::max<uint64_t>(1, nnz), s));
-  KC_CUDA(cudaMallocAsync(&dd, sizeof(uint32_t) * std::max<uint64_t>(1, nnz), s));
-  KC_CUDA(cudaMemcpyAsync(drp, row_ptr, sizeof(uint32_t) * ((size_t)n_nodes + 1), cudaMemcpyHostToDevice, s));
-  if (nnz) KC_CUDA(cudaMemcpyAsync(dd, col_ind, sizeof(uint32_t) * nnz, cudaMemcpyHostToDevice, s));
-  if (n_nodes)
-    kc::k_expand_rows<<<std::max(1u, std::min((n_nodes * 32u + 255u) / 256u, (uint32_t)ctx->sms * 32)), 256, 0, s>>>(
-        drp, n_nodes, ds);
-  kc_status st = kc::build_from_device(g, ds, dd, nnz, n_nodes);
-  cudaFreeAsync(drp, s);
-  cudaFreeAsync(ds, s);
-  cudaFreeAsync(dd, s);
+  kc_status st = KC_OK;
+  {
+    kc::DevTemps t(s);
+    uint32_t *drp = nullptr, *ds = nullptr, *dd = nullptr;
+    cudaError_t e = t.alloc(&drp, sizeof(uint32_t) * ((size_t)n_nodes + 1));
+    if (e == cudaSuccess) e = t.alloc(&ds, sizeof(uint32_t) * std::max<uint64_t>(1, nnz));
+    if (e == cudaSuccess) e = t.alloc(&dd, sizeof(uint32_t) * std::max<uint64_t>(1, nnz));
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(drp, row_ptr, sizeof(uint32_t) * ((size_t)n_nodes + 1), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && nnz) e = cudaMemcpyAsync(dd, col_ind, sizeof(uint32_t) * nnz, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && n_nodes)
+      kc::k_expand_rows<<<std::max(1u, std::min((n_nodes * 32u + 255u) / 256u, (uint32_t)ctx->sms * 32)), 256, 0,
+                          s>>>(drp, n_nodes, ds);
+    st = e == cudaSuccess ? kc::build_from_device(g, ds, dd, nnz, n_nodes)
+                          : kc::cuda_fail(e, "CSR staging", __FILE__, __LINE__);
+  }
   if (st != KC_OK) {
     kc::free_graph_arrays(g);
     delete g;
@@ -397,21 +358,33 @@ kc_status kc_parse_spec(const char* spec, kc_params* io) {
 }
 
 kc_status kc_count(kc_graph* g, const kc_params* p, kc_u128* out, kc_count_stats* stats) {
-  if (!g || !p || !out) return fail(KC_ERR_INVALID_ARG, "NULL argument");
+  if (!g) return fail(KC_ERR_INVALID_ARG, "NULL argument");
+  return kc::count_on(g->ctx, g, p, out, stats);
+}
+
+}  // extern "C"
+
+namespace kc {
+
+kc_status count_on(kc_ctx* run, kc_graph* g, const kc_params* p, kc_u128* out, kc_count_stats* stats) {
+  if (!run || !g || !p || !out) return fail(KC_ERR_INVALID_ARG, "NULL argument");
   if (p->k < 1) return fail(KC_ERR_INVALID_ARG, "k must be >= 1");
   if (p->mode > KC_MODE_AUTO || p->unit > KC_UNIT_EDGE || p->encoding > KC_ENC_LIST)
     return fail(KC_ERR_INVALID_ARG, "unknown mode, unit or encoding");
   if (p->part != 0 && (p->part > 32 || (p->part & (p->part - 1))))
     return fail(KC_ERR_INVALID_ARG, "partition size %u is not one of 1,2,4,8,16,32", p->part);
   if (g->oriented < 0) return fail(KC_ERR_NOT_ORIENTED, "call kc_orient before kc_count");
-  kc::CtxLock lock(g->ctx);
+  if (run != g->ctx && run->device != g->ctx->device)
+    return fail(KC_ERR_INVALID_ARG, "a graph can only be counted by a context of its own device");
+  kc::CtxLock lock(run);
   if (stats) std::memset(stats, 0, sizeof(*stats));
   out->lo = out->hi = 0;
   if (p->k == 1) { out->lo = g->n; return KC_OK; }
   if (p->k == 2) { out->lo = g->m; return KC_OK; }
-  cudaStream_t s = g->ctx->stream;
+  cudaStream_t s = run->stream;
+  kc::DevTemps t(s);
   unsigned long long* d_out = nullptr;
-  KC_CUDA(cudaMallocAsync(&d_out, 2 * sizeof(unsigned long long), s));
+  KC_CUDA(t.alloc(&d_out, 2 * sizeof(unsigned long long)));
   KC_CUDA(cudaMemsetAsync(d_out, 0, 2 * sizeof(unsigned long long), s));
   kc::CountRequest req;
   req.k = p->k;
@@ -421,6 +394,7 @@ kc_status kc_count(kc_graph* g, const kc_params* p, kc_u128* out, kc_count_stats
   req.encoding = p->encoding;
   req.flags = p->flags;
   req.k_max = p->k;
+  req.ctx = run;
   kc_status st = kc::count_graph(g, req, d_out, (p->flags & KC_FLAG_STATS) ? stats : nullptr);
   unsigned long long h[2] = {0, 0};
   if (st == KC_OK) {
@@ -428,11 +402,23 @@ kc_status kc_count(kc_graph* g, const kc_params* p, kc_u128* out, kc_count_stats
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) st = kc::cuda_fail(e, "count readback", __FILE__, __LINE__);
   }
-  cudaFreeAsync(d_out, s);
   out->lo = h[0];
   out->hi = h[1];
   return st;
 }
+
+kc_status complete_for_sharing(kc_graph* g) {
+  if (!g) return fail(KC_ERR_INVALID_ARG, "graph is NULL");
+  if (g->oriented < 0) return fail(KC_ERR_NOT_ORIENTED, "orient the graph before sharing it");
+  kc::CtxLock lock(g->ctx);
+  KC_TRY(ensure_edge_rows(g));
+  KC_CUDA(cudaStreamSynchronize(g->ctx->stream));
+  return KC_OK;
+}
+
+}  // namespace kc
+
+extern "C" {
 
 kc_status kc_count_local(kc_graph* g, const kc_params* p, kc_u128* per_vertex, kc_u128* total) {
   if (!g || !p || !per_vertex) return fail(KC_ERR_INVALID_ARG, "NULL argument");
@@ -459,9 +445,10 @@ kc_status kc_count_local(kc_graph* g, const kc_params* p, kc_u128* per_vertex, k
     if (total) *total = {p->k == 1 ? (unsigned long long)n : (unsigned long long)g->m, 0};
     return KC_OK;
   }
+  kc::DevTemps t(s);
   unsigned long long *d_out = nullptr, *d_local = nullptr;
-  KC_CUDA(cudaMallocAsync(&d_out, 2 * sizeof(unsigned long long), s));
-  KC_CUDA(cudaMallocAsync(&d_local, 2 * sizeof(unsigned long long) * std::max<uint32_t>(1, n), s));
+  KC_CUDA(t.alloc(&d_out, 2 * sizeof(unsigned long long)));
+  KC_CUDA(t.alloc(&d_local, 2 * sizeof(unsigned long long) * std::max<uint32_t>(1, n)));
   KC_CUDA(cudaMemsetAsync(d_out, 0, 2 * sizeof(unsigned long long), s));
   KC_CUDA(cudaMemsetAsync(d_local, 0, 2 * sizeof(unsigned long long) * std::max<uint32_t>(1, n), s));
   kc::CountRequest req;
@@ -483,8 +470,6 @@ kc_status kc_count_local(kc_graph* g, const kc_params* p, kc_u128* per_vertex, k
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) st = kc::cuda_fail(e, "local count readback", __FILE__, __LINE__);
   }
-  cudaFreeAsync(d_out, s);
-  cudaFreeAsync(d_local, s);
   if (st != KC_OK) return st;
   // counters are indexed by rank label; the caller's array by vertex id
   for (uint32_t v = 0; v < n; ++v) per_vertex[v] = {loc[2 * (size_t)rank[v]], loc[2 * (size_t)rank[v] + 1]};
@@ -510,15 +495,15 @@ kc_status kc_truss_support(kc_graph* g, uint32_t* support) {
   if (!g || (g->m && !support)) return fail(KC_ERR_INVALID_ARG, "NULL argument");
   kc::CtxLock lock(g->ctx);
   cudaStream_t s = g->ctx->stream;
+  kc::DevTemps t(s);
   uint32_t* d = nullptr;
-  KC_CUDA(cudaMallocAsync(&d, sizeof(uint32_t) * std::max<uint64_t>(1, g->m), s));
+  KC_CUDA(t.alloc(&d, sizeof(uint32_t) * std::max<uint64_t>(1, g->m)));
   kc_status st = kc::truss_support(g, d);
   if (st == KC_OK && g->m) {
     cudaError_t e = cudaMemcpyAsync(support, d, sizeof(uint32_t) * g->m, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) st = kc::cuda_fail(e, "support readback", __FILE__, __LINE__);
   }
-  cudaFreeAsync(d, s);
   return st;
 }
 

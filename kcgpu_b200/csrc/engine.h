@@ -15,7 +15,7 @@ struct kc_ctx {
   cudaStream_t stream = nullptr;
   int sms = 148;
   int max_smem_optin = 227 * 1024;
-  uint64_t spin_budget = 0;
+  uint64_t time_limit_ns = 0;  // device time limit of a counting pass (0 = none)
   uint64_t total_mem = 0;
   std::mutex mu;  // one call at a time per context
   // exact binomial table C(r, c) as (lo, hi) pairs, rows [0, brows], cols [0, bcols]
@@ -80,11 +80,21 @@ struct CountRequest {
   uint32_t k_max = 0;
   // local counts (orientation mode): (lo, hi) per rank label, zeroed; null otherwise
   unsigned long long* d_local = nullptr;
+  // context whose stream, side streams and scratch run the count (null: the
+  // graph's own); another context of the same device may count a graph that
+  // is complete (oriented, edge rows built), which the count then only reads
+  kc_ctx* ctx = nullptr;
 };
 
 // Runs the counting stage; d_out holds n_graphs (lo, hi) pairs and must be zeroed.
 kc_status count_graph(kc_graph* g, const CountRequest& req, unsigned long long* d_out,
                       kc_count_stats* stats);
+// kc_count run by the context `run` (its stream, scratch and lock) on a graph
+// of the same device; the graph must be complete (see CountRequest::ctx).
+kc_status count_on(kc_ctx* run, kc_graph* g, const kc_params* p, kc_u128* out, kc_count_stats* stats);
+// Completes an oriented graph for counting by other contexts: builds every
+// array a count could create lazily and waits for the graph's stream.
+kc_status complete_for_sharing(kc_graph* g);
 
 kc_status truss_support(kc_graph* g, uint32_t* d_support);
 

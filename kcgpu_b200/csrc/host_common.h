@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -30,6 +31,41 @@ inline double now_ms() {
   using namespace std::chrono;
   return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
 }
+
+// Device temporaries of one call: allocated stream-ordered on s and freed,
+// stream-ordered, when the guard goes out of scope, so a call that fails half
+// way leaks nothing. free_now() hands one back early to lower the peak.
+class DevTemps {
+ public:
+  explicit DevTemps(cudaStream_t s) : s_(s) {}
+  ~DevTemps() {
+    for (void* p : ps_) cudaFreeAsync(p, s_);
+  }
+  DevTemps(const DevTemps&) = delete;
+  DevTemps& operator=(const DevTemps&) = delete;
+
+  template <class T>
+  cudaError_t alloc(T** p, size_t bytes) {
+    void* q = nullptr;
+    const cudaError_t e = cudaMallocAsync(&q, bytes ? bytes : 4, s_);
+    *p = static_cast<T*>(q);
+    if (e == cudaSuccess) ps_.push_back(q);
+    return e;
+  }
+
+  void free_now(void* p) {
+    for (size_t i = 0; i < ps_.size(); ++i)
+      if (ps_[i] == p) {
+        cudaFreeAsync(p, s_);
+        ps_.erase(ps_.begin() + (long)i);
+        return;
+      }
+  }
+
+ private:
+  cudaStream_t s_;
+  std::vector<void*> ps_;
+};
 
 }  // namespace kc
 

@@ -300,33 +300,33 @@ __global__ void __launch_bounds__(256) k_peel(PeelArgs a) {
 
 }  // namespace
 
-kc_status peel_graph(kc_graph* g) {
-  if (g->prio) return KC_OK;
+namespace {
+
+// The peel into prio / level (n >= 1); temporaries freed on every path.
+kc_status run_peel(kc_graph* g, uint32_t* prio, uint32_t* level) {
   kc_ctx* ctx = g->ctx;
   cudaStream_t s = ctx->stream;
   const uint32_t n = g->n;
-  KC_TRY(dev_alloc(g, (void**)&g->prio, sizeof(uint32_t) * std::max<size_t>(1, n)));
-  KC_TRY(dev_alloc(g, (void**)&g->level, sizeof(uint32_t) * std::max<size_t>(1, n)));
-  if (n == 0) { g->max_core = 0; return KC_OK; }
+  DevTemps t(s);
   int* deg = nullptr;
   uint32_t *removed = nullptr, *inb = nullptr, *ba = nullptr, *bb = nullptr, *fa = nullptr, *fb = nullptr,
            *ctr = nullptr;
-  KC_CUDA(cudaMallocAsync(&deg, sizeof(int) * n, s));
-  KC_CUDA(cudaMallocAsync(&removed, sizeof(uint32_t) * n, s));
-  KC_CUDA(cudaMallocAsync(&inb, sizeof(uint32_t) * n, s));
-  KC_CUDA(cudaMallocAsync(&ba, sizeof(uint32_t) * n, s));
-  KC_CUDA(cudaMallocAsync(&bb, sizeof(uint32_t) * n, s));
-  KC_CUDA(cudaMallocAsync(&fa, sizeof(uint32_t) * n, s));
-  KC_CUDA(cudaMallocAsync(&fb, sizeof(uint32_t) * n, s));
-  KC_CUDA(cudaMallocAsync(&ctr, sizeof(uint32_t) * 32, s));
+  KC_CUDA(t.alloc(&deg, sizeof(int) * n));
+  KC_CUDA(t.alloc(&removed, sizeof(uint32_t) * n));
+  KC_CUDA(t.alloc(&inb, sizeof(uint32_t) * n));
+  KC_CUDA(t.alloc(&ba, sizeof(uint32_t) * n));
+  KC_CUDA(t.alloc(&bb, sizeof(uint32_t) * n));
+  KC_CUDA(t.alloc(&fa, sizeof(uint32_t) * n));
+  KC_CUDA(t.alloc(&fb, sizeof(uint32_t) * n));
+  KC_CUDA(t.alloc(&ctr, sizeof(uint32_t) * 32));
   KC_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t) * 32, s));
   const uint32_t init_prio = (uint32_t)std::min<uint64_t>(2 * g->m, 0xffffffffull);
-  k_peel_init<<<grid_for(n, ctx->sms), 256, 0, s>>>(g->rp, n, init_prio, deg, g->prio, g->level, removed, inb);
+  k_peel_init<<<grid_for(n, ctx->sms), 256, 0, s>>>(g->rp, n, init_prio, deg, prio, level, removed, inb);
   KC_CUDA(cudaGetLastError());
 
   PeelArgs a;
   a.rp = g->rp; a.col = g->col; a.n = n; a.init_prio = init_prio;
-  a.deg = deg; a.prio = g->prio; a.level = g->level; a.removed = removed; a.inbucket = inb;
+  a.deg = deg; a.prio = prio; a.level = level; a.removed = removed; a.inbucket = inb;
   a.bucket_a = ba; a.bucket_b = bb; a.front_a = fa; a.front_b = fb; a.ctr = ctr; a.out = ctr + 16;
   int per_sm = 0;
   KC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_peel, 256, 0));
@@ -337,11 +337,31 @@ kc_status peel_graph(kc_graph* g) {
   uint32_t out[3] = {0, 0, 0};
   KC_CUDA(cudaMemcpyAsync(out, ctr + 16, sizeof(out), cudaMemcpyDeviceToHost, s));
   KC_CUDA(cudaStreamSynchronize(s));
-  cudaFreeAsync(deg, s); cudaFreeAsync(removed, s); cudaFreeAsync(inb, s);
-  cudaFreeAsync(ba, s); cudaFreeAsync(bb, s); cudaFreeAsync(fa, s); cudaFreeAsync(fb, s); cudaFreeAsync(ctr, s);
   if (out[2]) return fail(KC_ERR_INTERNAL, "peel did not converge (device error %u)", out[2]);
   g->max_core = out[0];
   g->peel_rounds = out[1];
+  return KC_OK;
+}
+
+}  // namespace
+
+// Peel priorities and core numbers of the graph; the graph keeps them only
+// when the whole peel succeeded.
+kc_status peel_graph(kc_graph* g) {
+  if (g->prio) return KC_OK;
+  const uint32_t n = g->n;
+  uint32_t *prio = nullptr, *level = nullptr;
+  KC_TRY(dev_alloc(g, (void**)&prio, sizeof(uint32_t) * std::max<size_t>(1, n)));
+  kc_status st = dev_alloc(g, (void**)&level, sizeof(uint32_t) * std::max<size_t>(1, n));
+  if (st == KC_OK && n == 0) g->max_core = 0;
+  else if (st == KC_OK) st = run_peel(g, prio, level);
+  if (st != KC_OK) {
+    dev_free(g, prio);
+    dev_free(g, level);
+    return st;
+  }
+  g->prio = prio;
+  g->level = level;
   return KC_OK;
 }
 
@@ -362,13 +382,14 @@ kc_status orient_graph(kc_graph* g, uint32_t orientation) {
   KC_TRY(dev_alloc(g, (void**)&g->drp, sizeof(uint32_t) * ((size_t)n + 1)));
   KC_TRY(dev_alloc(g, (void**)&g->dcol, sizeof(uint32_t) * std::max<uint64_t>(1, g->m)));
   const int vbits = bits_for(n ? n - 1 : 0);
+  DevTemps t(s);
   unsigned long long *keys = nullptr, *tmp = nullptr;
   uint32_t *odeg = nullptr, *ucnt = nullptr, *mx = nullptr;
-  KC_CUDA(cudaMallocAsync(&keys, sizeof(unsigned long long) * std::max<size_t>(1, n), s));
-  KC_CUDA(cudaMallocAsync(&tmp, sizeof(unsigned long long) * std::max<size_t>(1, n), s));
-  KC_CUDA(cudaMallocAsync(&odeg, sizeof(uint32_t) * ((size_t)n + 1), s));
-  KC_CUDA(cudaMallocAsync(&ucnt, sizeof(uint32_t) * ((size_t)n + 1), s));
-  KC_CUDA(cudaMallocAsync(&mx, sizeof(uint32_t), s));
+  KC_CUDA(t.alloc(&keys, sizeof(unsigned long long) * std::max<size_t>(1, n)));
+  KC_CUDA(t.alloc(&tmp, sizeof(unsigned long long) * std::max<size_t>(1, n)));
+  KC_CUDA(t.alloc(&odeg, sizeof(uint32_t) * ((size_t)n + 1)));
+  KC_CUDA(t.alloc(&ucnt, sizeof(uint32_t) * ((size_t)n + 1)));
+  KC_CUDA(t.alloc(&mx, sizeof(uint32_t)));
   KC_CUDA(cudaMemsetAsync(mx, 0, sizeof(uint32_t), s));
   int major_bits;
   const int graph_bits = g->vgraph_orig ? bits_for(g->n_graphs ? g->n_graphs - 1 : 0) : 0;
@@ -400,7 +421,6 @@ kc_status orient_graph(kc_graph* g, uint32_t orientation) {
   // out-lists in rank order (values are distinct, so dedup keeps them all)
   KC_CUDA(prim::segmented_sort_unique(g->drp, g->dcol, ucnt, n, max_out, s));
   KC_CUDA(cudaGetLastError());
-  cudaFreeAsync(keys, s); cudaFreeAsync(tmp, s); cudaFreeAsync(odeg, s); cudaFreeAsync(ucnt, s); cudaFreeAsync(mx, s);
   KC_CUDA(cudaStreamSynchronize(s));
   g->max_out = max_out;
   g->oriented = (int)orientation;
@@ -420,11 +440,12 @@ kc_status export_dag(kc_graph* g, uint32_t* h_rp, uint32_t* h_col) {
   kc_ctx* ctx = g->ctx;
   cudaStream_t s = ctx->stream;
   const uint32_t n = g->n;
+  DevTemps t(s);
   uint32_t *deg = nullptr, *orp = nullptr, *ocol = nullptr, *ucnt = nullptr;
-  KC_CUDA(cudaMallocAsync(&deg, sizeof(uint32_t) * ((size_t)n + 1), s));
-  KC_CUDA(cudaMallocAsync(&orp, sizeof(uint32_t) * ((size_t)n + 1), s));
-  KC_CUDA(cudaMallocAsync(&ocol, sizeof(uint32_t) * std::max<uint64_t>(1, g->m), s));
-  KC_CUDA(cudaMallocAsync(&ucnt, sizeof(uint32_t) * ((size_t)n + 1), s));
+  KC_CUDA(t.alloc(&deg, sizeof(uint32_t) * ((size_t)n + 1)));
+  KC_CUDA(t.alloc(&orp, sizeof(uint32_t) * ((size_t)n + 1)));
+  KC_CUDA(t.alloc(&ocol, sizeof(uint32_t) * std::max<uint64_t>(1, g->m)));
+  KC_CUDA(t.alloc(&ucnt, sizeof(uint32_t) * ((size_t)n + 1)));
   k_export_deg<<<grid_for(n, ctx->sms), 256, 0, s>>>(g->drp, g->rank, n, deg);
   KC_CUDA(prim::scan_exclusive_u32(deg, orp, n, s));
   k_export_fill<<<grid_for((uint64_t)n * 32, ctx->sms, 32), 256, 0, s>>>(g->drp, g->dcol, g->rank, g->inv, n, orp, ocol);
@@ -432,7 +453,6 @@ kc_status export_dag(kc_graph* g, uint32_t* h_rp, uint32_t* h_col) {
   KC_CUDA(cudaMemcpyAsync(h_rp, orp, sizeof(uint32_t) * ((size_t)n + 1), cudaMemcpyDeviceToHost, s));
   if (g->m) KC_CUDA(cudaMemcpyAsync(h_col, ocol, sizeof(uint32_t) * g->m, cudaMemcpyDeviceToHost, s));
   KC_CUDA(cudaStreamSynchronize(s));
-  cudaFreeAsync(deg, s); cudaFreeAsync(orp, s); cudaFreeAsync(ocol, s); cudaFreeAsync(ucnt, s);
   return KC_OK;
 }
 

@@ -1,16 +1,17 @@
 // Continuous-batching request server for clique-count queries.
 //
 // No counterpart in the reference (one graph per process, results printed).
-// Requests (a resident graph + k, or a one-shot edge list + k) enter a FIFO.
-// W worker threads, each with its own context and CUDA stream, take the head
-// of the queue as soon as (a) a worker is free and (b) the request's projected
-// device footprint fits in the HBM budget next to the resident graphs and the
-// requests already on the device. Requests therefore start while others are
-// still running, and their kernels overlap on the device through the workers'
-// streams. A worker that takes a one-shot request also takes the one-shot
-// requests queued right behind it (up to 512 requests / 8M edges, within the
-// budget) and counts them in one batched call. Results are exact integers, so
-// a request's count is the same alone and in any mix.
+// Requests (a resident graph + k, or a one-shot edge list + k) enter a queue.
+// W worker threads, each with its own context and CUDA stream, take the first
+// queued request whose projected device footprint fits in the HBM budget next
+// to the resident graphs and the requests already on the device, as soon as a
+// worker is free (a blocked head can be passed only while it is young, see
+// admissible()). Requests therefore start while others are still running,
+// and their kernels overlap on the device through the workers' streams. A
+// worker that takes a one-shot request also takes the other queued one-shot
+// requests that fit (up to 512 requests / 8M edges) and counts them in one
+// batched call. Results are exact integers, so a request's count is the same
+// alone and in any mix.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -31,11 +32,13 @@
 
 namespace {
 
+// A resident graph is complete (oriented, edge rows built) before any request
+// sees it, so requests only read it: any worker counts it on its own context
+// and stream, several at a time.
 struct Resident {
   kc_graph* g = nullptr;
   uint64_t bytes = 0;
   kc_graph_info info{};
-  std::mutex mu;  // one request at a time per resident graph
   ~Resident() {
     if (g) kc_graph_destroy(g);
   }
@@ -105,10 +108,9 @@ void execute(kc_server* s, kc_ctx* ctx, Request& r) {
     if (!res) {
       st = kc::fail(KC_ERR_INVALID_ARG, "graph %llu is not resident", (unsigned long long)r.graph_id);
     } else {
-      std::lock_guard<std::mutex> gl(res->mu);
       kc_params p = choose(s, res->info, r.k);
       r.res.params = p;
-      st = kc_count(res->g, &p, &out, nullptr);
+      st = kc::count_on(ctx, res->g, &p, &out, nullptr);
     }
   } else {
     kc_graph* g = nullptr;
@@ -165,33 +167,63 @@ void execute_batch(kc_server* s, kc_ctx* ctx, std::vector<std::shared_ptr<Reques
   }
 }
 
+// Admission: the first queued request whose projected footprint fits next to
+// the resident graphs and the requests already running (any request when
+// nothing runs, so a request as large as the whole budget still starts).
+// Requests behind a blocked head may pass it, but only while the head is
+// younger than kHeadAgeMs: after that nothing passes it, the device drains
+// and the head starts, so a large request is not starved by a stream of
+// small ones.
+constexpr double kHeadAgeMs = 250.0;
+
+std::deque<std::shared_ptr<Request>>::iterator admissible(kc_server* s) {
+  auto fits = [&](const Request& r) {
+    return s->inflight_bytes == 0 || s->resident_bytes + s->inflight_bytes + r.footprint <= s->budget;
+  };
+  if (s->queue.empty()) return s->queue.end();
+  if (fits(*s->queue.front())) return s->queue.begin();
+  if (s->ms() - s->queue.front()->res.submit_ms > kHeadAgeMs) return s->queue.end();
+  for (auto it = s->queue.begin() + 1; it != s->queue.end(); ++it)
+    if (fits(**it)) return it;
+  return s->queue.end();
+}
+
 void worker_main(kc_server* s, size_t wi) {
   kc_ctx* ctx = s->wctx[wi];
   for (;;) {
     std::vector<std::shared_ptr<Request>> rs;
     {
       std::unique_lock<std::mutex> l(s->mu);
-      s->cv_work.wait(l, [&]() {
-        if (s->stop) return true;
-        if (s->queue.empty()) return false;
-        const uint64_t fp = s->queue.front()->footprint;
-        return s->inflight_bytes == 0 || s->resident_bytes + s->inflight_bytes + fp <= s->budget;
-      });
+      auto pick = s->queue.end();
+      // a blocked head that comes of age needs no event, so the wait wakes
+      // up now and then to look again
+      while (!s->stop && (pick = admissible(s)) == s->queue.end())
+        s->cv_work.wait_for(l, std::chrono::milliseconds(20));
       if (s->stop) return;
       uint64_t edges = 0;
-      do {
-        std::shared_ptr<Request> r = s->queue.front();
-        s->queue.pop_front();
+      auto take = [&](std::deque<std::shared_ptr<Request>>::iterator it) {
+        std::shared_ptr<Request> r = *it;
+        s->queue.erase(it);
         s->inflight_bytes += r->footprint;
         r->running = true;
         r->res.start_ms = s->ms();
         edges += r->src.size();
         rs.push_back(std::move(r));
-        if (rs.front()->graph_id) break;  // resident graphs run on their own
-      } while (!s->queue.empty() && rs.size() < kBatchMaxRequests && s->queue.front()->graph_id == 0 &&
-               s->queue.front()->k >= 3 && rs.front()->k >= 3 &&
-               edges + s->queue.front()->src.size() <= kBatchMaxEdges &&
-               s->resident_bytes + s->inflight_bytes + s->queue.front()->footprint <= s->budget);
+      };
+      take(pick);
+      // one-shot requests (k >= 3) queued anywhere behind it join it in one
+      // batched call while they fit
+      if (rs.front()->graph_id == 0 && rs.front()->k >= 3) {
+        size_t i = 0;  // (erase invalidates deque iterators: walk by index)
+        while (i < s->queue.size() && rs.size() < kBatchMaxRequests) {
+          const Request& r = *s->queue[i];
+          if (r.graph_id == 0 && r.k >= 3 && edges + r.src.size() <= kBatchMaxEdges &&
+              s->resident_bytes + s->inflight_bytes + r.footprint <= s->budget)
+            take(s->queue.begin() + (long)i);  // the next request moves up to index i
+          else
+            ++i;
+        }
+      }
     }
     if (rs.size() == 1) execute(s, ctx, *rs[0]);
     else execute_batch(s, ctx, rs);
@@ -305,6 +337,7 @@ kc_status kc_server_put_graph(kc_server* s, const uint32_t* src, const uint32_t*
   auto res = std::make_shared<Resident>();
   KC_TRY(kc_graph_from_edges(owner, src, dst, n_edges, n_nodes, &res->g));
   KC_TRY(kc_orient(res->g, s->opts.orientation));
+  KC_TRY(kc::complete_for_sharing(res->g));
   kc_graph_get_info(res->g, &res->info);
   res->bytes = res->info.device_bytes;
   std::lock_guard<std::mutex> l(s->mu);

@@ -70,17 +70,16 @@ kc_status truss_support(kc_graph* g, uint32_t* d_support) {
   cudaStream_t s = ctx->stream;
   const uint32_t n = g->n;
   if (g->m == 0) return KC_OK;
+  DevTemps t(s);
   uint32_t *cnt = nullptr, *ubase = nullptr;
-  KC_CUDA(cudaMallocAsync(&cnt, sizeof(uint32_t) * ((size_t)n + 1), s));
-  KC_CUDA(cudaMallocAsync(&ubase, sizeof(uint32_t) * ((size_t)n + 1), s));
+  KC_CUDA(t.alloc(&cnt, sizeof(uint32_t) * ((size_t)n + 1)));
+  KC_CUDA(t.alloc(&ubase, sizeof(uint32_t) * ((size_t)n + 1)));
   const uint32_t g1 = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->sms * 16));
   k_upper_count<<<g1, 256, 0, s>>>(g->rp, g->col, n, cnt);
   KC_CUDA(prim::scan_exclusive_u32(cnt, ubase, n, s));
   const uint32_t g2 = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((g->m * 32 + 255) / 256, (uint64_t)ctx->sms * 32));
   k_support<<<g2, 256, 0, s>>>(g->rp, g->col, n, ubase, (uint32_t)g->m, d_support);
   KC_CUDA(cudaGetLastError());
-  cudaFreeAsync(cnt, s);
-  cudaFreeAsync(ubase, s);
   return KC_OK;
 }
 

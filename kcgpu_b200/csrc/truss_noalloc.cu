@@ -25,7 +25,10 @@
 //     caller;
 //   * the first call on each device looks up the array's device address
 //     (cudaGetSymbolAddress, with that device current) and caches it; make
-//     that first call before any stream capture begins.
+//     that first call before any stream capture begins;
+//   * the cached address belongs to the device's primary context: after
+//     cudaDeviceReset (which destroys that context and the array in it) this
+//     entry point must not be called again in the process.
 #include <algorithm>
 #include <mutex>
 

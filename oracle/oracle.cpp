@@ -308,6 +308,17 @@ struct PivotCounter {
   }
 };
 
+// Vertices by decreasing out-degree (ties by id): the units a thread pool
+// should take first, so the largest ones do not end up in the tail.
+std::vector<uint32_t> heavy_first(const or_graph* g) {
+  std::vector<uint32_t> order(g->n);
+  for (uint32_t v = 0; v < g->n; ++v) order[v] = v;
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+    return g->drp[a + 1] - g->drp[a] > g->drp[b + 1] - g->drp[b];
+  });
+  return order;
+}
+
 void peel(or_graph* g) {
   // Level-synchronous peeling with the reference's sub-round priorities.
   const uint32_t n = g->n;
@@ -469,14 +480,16 @@ int or_count_ex(const or_graph* g, uint32_t k, int mode, int unit, int threads, 
     for (uint32_t v = 0; v < n; ++v) maxd = std::max(maxd, g->drp[v + 1] - g->drp[v]);
     Binom B;
     B.build(maxd + 1, k);
+    const std::vector<uint32_t> order = heavy_first(g);
 #pragma omp parallel num_threads(nt)
     {
       u128 local = 0;
       OrientCounter oc(*g, k + 1);
       PivotCounter pc(k, B);
       pc.closed = (flags & 1) != 0;
-#pragma omp for schedule(dynamic, 16)
-      for (int64_t v = 0; v < (int64_t)n; ++v) {
+#pragma omp for schedule(dynamic, 1)
+      for (int64_t oi = 0; oi < (int64_t)n; ++oi) {
+        const uint32_t v = order[oi];
         uint32_t d = g->drp[v + 1] - g->drp[v];
         if (d < t) continue;
         const uint32_t* nv = g->dcol.data() + g->drp[v];
@@ -499,6 +512,7 @@ int or_count_ex(const or_graph* g, uint32_t k, int mode, int unit, int threads, 
     for (uint32_t v = 0; v < n; ++v) maxd = std::max(maxd, g->drp[v + 1] - g->drp[v]);
     Binom B;
     B.build(maxd + 1, k);
+    const std::vector<uint32_t> order = heavy_first(g);
 #pragma omp parallel num_threads(nt)
     {
       u128 local = 0;
@@ -506,8 +520,9 @@ int or_count_ex(const or_graph* g, uint32_t k, int mode, int unit, int threads, 
       PivotCounter pc(k, B);
       pc.closed = (flags & 1) != 0;
       std::vector<uint32_t> tri;
-#pragma omp for schedule(dynamic, 16)
-      for (int64_t u = 0; u < (int64_t)n; ++u) {
+#pragma omp for schedule(dynamic, 1)
+      for (int64_t oi = 0; oi < (int64_t)n; ++oi) {
+        const uint32_t u = order[oi];
         const uint32_t* nu = g->dcol.data() + g->drp[u];
         uint32_t du = g->drp[u + 1] - g->drp[u];
         for (uint32_t i = 0; i < du; ++i) {
