@@ -37,6 +37,10 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "graphs/s, batched exact k-clique counts (10,000 mixed small graphs, k 4-12)"
 UNIT = "graphs/s"
+# DRAM bytes (read + write) of one step's counting launches, from the ncu
+# capture summarised in the file named below; None until captured.
+COUNT_DRAM_BYTES_PER_STEP = None
+COUNT_DRAM_SOURCE = None
 
 
 def parse():
@@ -301,7 +305,9 @@ def max_over_ranks(pg, x: float, device) -> float:
 
 
 def make_batch(kc, n_graphs: int, seed: int, pinned: bool = True):
-    el = kc.gen_batch(n_graphs, seed, pinned=pinned)
+    """The seeded batch; pageable batches come from the generator-only library,
+    so a process that only runs the CPU reference never loads the engine."""
+    el = kc.gen_batch(n_graphs, seed, pinned=True) if pinned else kc.gen_batch_host(n_graphs, seed)
     s, d, _ = el.arrays(copy=False)  # views of the generator's (page-locked when pinned) arrays
     off, nn, kk, fam = el.batch_meta()
     return el, s, d, off, nn, kk, fam
@@ -411,16 +417,22 @@ def main():
     clocks.start()
     l0 = L.kc_kernel_launches()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    stage = {"ms_h2d": [], "ms_build": [], "ms_count": []}
+    stage = {"ms_h2d": [], "ms_build": [], "ms_csr": [], "ms_orient": [], "ms_count": [], "ms_host_total": []}
     trav = {"tree_nodes": 0, "word_ops": 0, "gather_bytes": 0, "heavy_units": 0}
+    cycles = [0, 0, 0]
+    host_ms = [0.0] * 5
+    sizes = {}
     for i in range(args.steps):
         evs[i][0].record(stream)
         counts, choice, st = run_device()
         evs[i][1].record(stream)
         for key in stage:
-            stage[key].append(st[key])
+            stage[key].append(st["ms_total" if key == "ms_host_total" else key])
         for key in trav:
             trav[key] += st[key]
+        cycles = [a + b for a, b in zip(cycles, st["cycles"])]
+        host_ms = [a + b / args.steps for a, b in zip(host_ms, st["host_ms"])]
+        sizes = {"vertices": st["n_vertices"], "edges_dedup": st["n_edges"]}
     torch.cuda.synchronize()
     launches = (L.kc_kernel_launches() - l0) // max(1, args.steps)
     clk = clocks.stop()
@@ -473,29 +485,50 @@ def main():
                    "bitexact": bitexact_cpu}
         h2d = 8 * E + 8 * (G + 1) + 8 * G
         ms_count = sum(stage["ms_count"]) / len(stage["ms_count"])
-        # Roofline of the dominant stage, the counting launch (k_count_bitmap):
-        # its algorithmic HBM bytes are the adjacency lists gathered to build
-        # the induced subgraphs (measured by the kernels' counters); the
-        # traversal itself runs from shared memory, so the word-op figure is
-        # given beside it against the POPC issue rate (16 per SM per clock).
+        ms_build = sum(stage["ms_build"]) / len(stage["ms_build"])
         peaks = {}
         try:
             peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
         except (OSError, ValueError):
             pass
         hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+        peak_src = "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s (of fallback)"
         steps = max(1, args.steps)
+        # Counting launch (k_count_bitmap, every counting kernel of a step).
+        # Its algorithmic HBM bytes are the out-lists gathered to build the
+        # induced subgraphs, 4 (|S| + sum of |N+(v)| over v in S) per unit,
+        # counted by the kernels; DRAM traffic per step comes from the ncu
+        # capture summarised in profiles/ (most of the gather hits L2).
         gb_s = (trav["gather_bytes"] / steps) / (ms_count / 1e3) / 1e9
         sm_mhz = (clk.get("sm_mhz") or 1965.0)
         popc_peak = 16 * 148 * sm_mhz * 1e6
         wops = (trav["word_ops"] / steps) / (ms_count / 1e3)
+        tot_cy = max(1.0, float(sum(cycles)))
         roofline = {"bound": "hbm", "kernel": "k_count_bitmap (all counting launches of a step)",
                     "achieved": gb_s, "peak": hbm_peak, "unit": "GB/s", "frac": gb_s / hbm_peak,
-                    "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s",
-                    "algorithmic_bytes_per_step": trav["gather_bytes"] / steps, "traffic": None,
-                    "word_ops_per_s": wops, "popc_peak_per_s": popc_peak, "popc_frac": wops / popc_peak,
-                    "tree_nodes_per_step": trav["tree_nodes"] / steps,
-                    "heavy_units_per_step": trav["heavy_units"] / steps}
+                    "peak_source": peak_src, "algorithmic_bytes_per_step": trav["gather_bytes"] / steps,
+                    "traffic": COUNT_DRAM_BYTES_PER_STEP,
+                    "traffic_source": COUNT_DRAM_SOURCE,
+                    "limiter": "not HBM: latency and integer issue of the gather and traversal (roofline_issue)"}
+        # The same launch against its real limiter: where its unit groups spend
+        # their cycles, and its AND+POPC word-operation rate against the POPC
+        # issue rate (16 per SM per clock at the sampled SM clock).
+        roofline_issue = {"bound": "int-issue", "kernel": "k_count_bitmap", "achieved": wops, "peak": popc_peak,
+                          "unit": "word-ops/s", "frac": wops / popc_peak,
+                          "group_cycle_share": {"form_S": cycles[0] / tot_cy, "gather_subgraph": cycles[1] / tot_cy,
+                                                "traverse": cycles[2] / tot_cy},
+                          "tree_nodes_per_step": trav["tree_nodes"] / steps,
+                          "heavy_units_per_step": trav["heavy_units"] / steps}
+        # CSR build + orientation: algorithmic bytes = read the input pairs
+        # (8 E), write the symmetric CSR (8 m + 4 (n + 1)), read it again for the
+        # orientation (8 m + 4 (n + 1)) and write the DAG (4 m + 4 (n + 1)).
+        nv, mm = sizes.get("vertices", 0), sizes.get("edges_dedup", 0)
+        build_bytes = 8 * E + 20 * mm + 12 * (nv + 1)
+        roofline_build = {"bound": "hbm", "kernel": "CSR build + degree orientation (csr.cu, prims.cu, orient.cu)",
+                          "achieved": build_bytes / (ms_build / 1e3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                          "frac": build_bytes / (ms_build / 1e3) / 1e9 / hbm_peak, "peak_source": peak_src,
+                          "algorithmic_bytes_per_step": build_bytes,
+                          "ms": {"csr": sum(stage["ms_csr"]) / steps, "orient": sum(stage["ms_orient"]) / steps}}
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_step, "higher_is_better": True, "scaling": "weak",
@@ -515,6 +548,10 @@ def main():
             "clocks": clk,
             "cpu_baseline": cpu,
             "roofline": roofline,
+            "roofline_issue": roofline_issue,
+            "roofline_build": roofline_build,
+            "host_ms": {"checks_h2d": host_ms[0], "build": host_ms[1], "plan": host_ms[2], "count": host_ms[3],
+                        "readback": host_ms[4]},
         }
     if rank == 0:
         print(json.dumps(out), flush=True)

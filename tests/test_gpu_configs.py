@@ -1,93 +1,85 @@
-"""The single-graph configurations at full size.
+"""The benchmark configurations at full size, against exact fixtures.
 
-At full size the CPU oracle would take minutes, so these tests check
-size-independent properties: every algorithm (orientation listing, pivoting,
-node and edge units) gives the same exact count, and planted cliques bound the
-count from below. The same generators at a smaller scale are compared with the
-oracle exactly.
+tests/golden/configs.json holds the CPU oracle's counts for each
+configuration (tests/golden/make_config_golden.py, OpenMP, no GPU), with the
+sha256 of the generator's output, so the engine is compared with an
+independent count, not with its own other algorithms:
+
+  plain_small  ER G(2000, 0.01) seed 1, degree orientation, orientation mode,
+               node units, partition 8, binary encoding, k = 3, 4
+  rmat18/20    R-MAT scale 18 / 20, edge factor 16, (0.57, 0.19, 0.19, 0.05),
+               degeneracy orientation, pivoting, edge units, partition 8,
+               binary encoding, k = 5, 7 (as far as the oracle went)
+  chunglu4m    Chung-Lu n = 4M + 200 planted cliques of 30-60, degeneracy,
+               pivoting, k = 3.. (as far as the oracle went)
+  batch10k     the bench's 10,000-graph batch: every graph's count
+Every available k is checked; a configuration the fixture does not hold yet
+is skipped with the reason.
 """
+import hashlib
+import json
 import math
+import sys
+from pathlib import Path
 
+import numpy as np
 import pytest
 
 import kcgpu_b200 as kc
-from oracle.oracle import OracleGraph
 
 pytestmark = pytest.mark.gpu
 
+GOLDEN = Path(__file__).resolve().parent / "golden"
+sys.path.insert(0, str(GOLDEN))
+import make_config_golden as MCG  # noqa: E402
 
-def test_rmat_scale16_matches_oracle(ctx):
-    # the CPU Pivoter needs ~10 s here at k = 5 (minutes at k = 7), so k = 7 is
-    # checked as agreement between the engine's algorithms
-    s, d, n = kc.gen_rmat(16, 16, 0.57, 0.19, 0.19, seed=20).arrays()
-    og = OracleGraph(s, d, n)
-    og.orient("degen")
+
+def _fixture(name):
+    fx = json.loads((GOLDEN / "configs.json").read_text())["configs"]
+    if name not in fx or not fx[name].get("counts"):
+        pytest.skip(f"{name}: not in tests/golden/configs.json yet")
+    return fx[name]
+
+
+def _check_single(ctx, name, mode, unit, part):
+    rec = _fixture(name)
+    _, s, d, n, orient, _, _ = MCG.graph_spec(name)
+    assert MCG.sha_arrays(s, d) == rec["input_sha256"], f"{name}: generator output changed"
     with kc.Graph.from_edges(ctx, s, d, n) as g:
-        g.orient("degen")
-        want = og.count(5, "pivot", "node")
-        assert g.count(5, mode="pivot", unit="edge", part=8, encoding="bitmap") == want
-        assert g.count(5, mode="auto", unit="node", part=0) == want
-        assert g.count(5, mode="orient", unit="node", part=0) == want
-        c7 = g.count(7, mode="pivot", unit="edge", part=8, encoding="bitmap")
-        assert g.count(7, mode="pivot", unit="node", part=0) == c7
-        assert g.count(7, mode="auto", unit="edge", part=0) == c7
+        g.orient(orient)
+        assert g.info()["m"] == rec["m"]
+        for k, want in rec["counts"].items():
+            got = g.count(int(k), mode=mode, unit=unit, part=part, encoding="bitmap")
+            assert got == int(want), (name, k, got, want)
+    return rec
+
+
+def test_plain_small_er(ctx):
+    _check_single(ctx, "plain_small", "orient", "node", 8)
+
+
+def test_rmat_scale18(ctx):
+    _check_single(ctx, "rmat18", "pivot", "edge", 8)
 
 
 def test_rmat_scale20_edge_factor16(ctx):
-    # R-MAT scale 20, edge factor 16, (a,b,c,d) = (0.57,0.19,0.19,0.05), degeneracy
-    # orientation, pivoting on edge units with partition 8 and bitmaps. k = 5 here
-    # (about a second per algorithm); k = 7 expands ~7e10 clique-tree nodes
-    # (minutes), so it is timed by the benchmark's config leg instead.
-    s, d, n = kc.gen_rmat(20, 16, 0.57, 0.19, 0.19, seed=1).arrays()
-    with kc.Graph.from_edges(ctx, s, d, n) as g:
-        g.orient("degen")
-        info = g.info()
-        assert info["n"] == 1 << 20 and 10_000_000 < info["m"] < 16_000_000
-        ref = g.count(5, mode="pivot", unit="edge", part=8, encoding="bitmap")
-        assert ref > 0
-        assert g.count(5, mode="pivot", unit="node", part=8) == ref
-        assert g.count(5, mode="auto", unit="node", part=0) == ref
-
-
-def test_rmat_scale18_k7(ctx):
-    s, d, n = kc.gen_rmat(18, 16, 0.57, 0.19, 0.19, seed=1).arrays()
-    with kc.Graph.from_edges(ctx, s, d, n) as g:
-        g.orient("degen")
-        ref = g.count(7, mode="pivot", unit="edge", part=8, encoding="bitmap")
-        assert ref > 0
-        assert g.count(7, mode="pivot", unit="node", part=0) == ref
+    rec = _check_single(ctx, "rmat20", "pivot", "edge", 8)
+    assert rec["n_nodes"] == 1 << 20 and 10_000_000 < rec["m"] < 16_000_000
 
 
 def test_chung_lu_4m_planted_cliques(ctx):
-    # Chung-Lu, exponent 2.1, n = 4M, mean degree 20, degree cap 50k, plus 200
-    # planted cliques of 30-60 vertices; pivoting, 128-bit counts. k = 3 and 6
-    # here; k = 9 and 12 expand 1e10+ tree nodes (tens of seconds to minutes)
-    # and are timed by the benchmark's config leg; the smaller Chung-Lu test
-    # below checks k up to 12 against the oracle.
-    el = kc.gen_chung_lu(4_000_000, 2.1, 20.0, 50_000.0, 3)
-    el.plant_cliques(200, 30, 60, 11)
-    s, d, n = el.arrays()
-    with kc.Graph.from_edges(ctx, s, d, n) as g:
-        g.orient("degen")
-        core, mx = g.kcore()
-        assert mx >= 29  # every planted clique of s vertices is an (s-1)-core
-        for k in (3, 6):
-            a = g.count(k, mode="pivot", unit="node", part=0)
-            b = g.count(k, mode="pivot", unit="edge", part=0)
-            assert a == b
-            assert g.count(k, mode="auto", unit="node", part=0) == a
+    rec = _check_single(ctx, "chunglu4m", "pivot", "node", 0)
+    for k, want in rec["counts"].items():
+        assert int(want) >= 200 * math.comb(30, int(k))  # 200 disjoint planted cliques of >= 30 vertices
 
 
-def test_chung_lu_small_planted_matches_oracle(ctx):
-    el = kc.gen_chung_lu(100_000, 2.1, 20.0, 2_000.0, 5)
-    el.plant_cliques(10, 30, 40, 7)
-    s, d, n = el.arrays()
-    og = OracleGraph(s, d, n)
-    og.orient("degen")
-    with kc.Graph.from_edges(ctx, s, d, n) as g:
-        g.orient("degen")
-        for k in (3, 6, 9, 12):
-            want = og.count(k, "pivot")
-            assert want >= 10 * math.comb(30, k)  # ten disjoint planted cliques of >= 30 vertices
-            assert g.count(k, mode="pivot", unit="node", part=0) == want
-            assert g.count(k, mode="pivot", unit="edge", part=8) == want
+def test_batch_of_10000_graphs(ctx):
+    rec = _fixture("batch10k")
+    el = kc.gen_batch(MCG.BATCH_GRAPHS, MCG.BATCH_SEED)
+    s, d, _ = el.arrays(copy=False)
+    off, nn, kk, fam = el.batch_meta()
+    assert MCG.sha_arrays(s, d, off, nn, kk, fam) == rec["input_sha256"]
+    got = kc.batch_count(ctx, s, d, off, nn, kk, orientation="degree", autotune=True)
+    want = [int(c) for c in rec["counts"]]
+    bad = [i for i, (a, b) in enumerate(zip(got, want)) if a != b]
+    assert len(got) == len(want) and not bad, f"{len(bad)} graphs differ, first {bad[:5]}"

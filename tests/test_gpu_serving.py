@@ -41,6 +41,41 @@ def test_mixed_requests_match_lone_counts(ctx):
             assert r["submit_ms"] <= r["start_ms"] <= r["done_ms"]
 
 
+def test_requests_overlap_on_the_device(ctx):
+    # four resident graphs (each owned by another worker context) and eight
+    # requests: a later request starts while an earlier one is still running
+    graphs = [kc.gen_rmat(14, 16, seed=30 + i).arrays() for i in range(4)]
+    with kc.Server(ctx, streams=4) as srv:
+        ids = [srv.put_graph(s, d, n) for s, d, n in graphs]
+        tickets = [(srv.submit(ids[i % 4], 7), i % 4) for i in range(8)]
+        res = [(srv.wait(t), gi) for t, gi in tickets]
+    overlapped = any(b["start_ms"] < a["done_ms"] and a["start_ms"] <= b["start_ms"]
+                     for i, (a, _) in enumerate(res) for (b, _) in res[i + 1:])
+    assert overlapped, [(r["start_ms"], r["done_ms"]) for r, _ in res]
+    want = {gi: _alone(ctx, *graphs[gi], 7) for gi in range(4)}
+    for r, gi in res:
+        assert r["count"] == want[gi]
+
+
+def test_admission_passes_a_blocked_head(ctx):
+    # The budget holds the large request A and a small one, not two large
+    # ones: B (large, behind A) must wait, C (small, behind B) passes it.
+    big = kc.gen_rmat(15, 16, seed=7).arrays()
+    small = kc.gen_er(400, 0.05, 8).arrays()
+    fp_big = kc.footprint_bytes(big[2], len(big[0]), 0)
+    fp_small = kc.footprint_bytes(small[2], len(small[0]), 0)
+    budget = fp_big + fp_small + (fp_big - fp_small) // 2
+    with kc.Server(ctx, hbm_budget_bytes=budget, streams=4) as srv:
+        ta = srv.submit_edges(*big, 8)
+        tb = srv.submit_edges(*big, 8)
+        tc = srv.submit_edges(*small, 4)
+        a, b, c = srv.wait(ta), srv.wait(tb), srv.wait(tc)
+    assert c["start_ms"] < b["start_ms"]
+    assert b["start_ms"] >= a["done_ms"]  # never two large requests on the device at once
+    assert a["count"] == b["count"] == _alone(ctx, *big, 8)
+    assert c["count"] == _alone(ctx, *small, 4)
+
+
 def test_cancel_and_admission(ctx):
     s, d, n = kc.gen_rmat(13, 16, seed=1).arrays()
     with kc.Server(ctx, streams=1) as srv:

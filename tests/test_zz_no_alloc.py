@@ -39,16 +39,22 @@ def _noalloc_support(ctx, g):
 
 
 def test_noalloc_truss_support_matches_allocating_entry_point():
+    from oracle.oracle import OracleGraph
+
     ctx = kc.Context(0)
     try:
         first = kc.gen_er(3000, 0.01, 17).arrays()
         second = kc.gen_rmat(10, 8, seed=4).arrays()
-        for s, d, n in (first, second):
+        at_limit = kc.gen_er(1 << 18, 1e-5, 23).arrays()  # n_nodes at the array's limit, sparse
+        no_edges = (np.zeros(0, np.uint32), np.zeros(0, np.uint32), 5)
+        for s, d, n in (first, second, at_limit, no_edges):
             with kc.Graph.from_edges(ctx, s, d, n) as g:
+                assert g.info()["n"] == n
                 want = g.truss_support()
                 got = _noalloc_support(ctx, g)
                 assert got.shape == want.shape
                 assert np.array_equal(got, want)
+                assert np.array_equal(got, OracleGraph(s, d, n).truss_support())
     finally:
         ctx.close()
 
