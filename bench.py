@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--requests", type=int, default=128)
     ap.add_argument("--rate", type=float, default=2000.0)
     ap.add_argument("--serve-max-edges", type=float, default=1e5)
+    ap.add_argument("--streams", type=int, default=8, help="serving: worker contexts / streams")
+    ap.add_argument("--no-serving", action="store_true", help="batched workload: skip the serving leg")
     return ap.parse_args()
 
 
@@ -90,19 +92,28 @@ def serving_requests(kc, n_req: int, seed: int, max_edges: float = 1e5):
 
 
 def run_serving(args):
-    """Continuous batching: requests arrive by a Poisson process at args.rate
-    per second and are submitted as they arrive; latency = done - arrival."""
+    """The serving configuration on its own (one JSON line)."""
     import torch
 
     import kcgpu_b200 as kc
 
     torch.cuda.set_device(0)
     ctx = kc.Context(0)
+    line = serving_leg(kc, ctx, args)
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def serving_leg(kc, ctx, args):
+    """Continuous batching: requests arrive by a Poisson process at args.rate
+    per second and are submitted as they arrive; latency = done - submission
+    (server clock). The same requests then run one per call on the plain path
+    in arrival order; both sets of counts must agree exactly."""
     resident, reqs = serving_requests(kc, args.requests, args.seed, args.serve_max_edges)
     rng = np.random.default_rng(args.seed + 1)
     gaps = rng.exponential(1.0 / args.rate, size=len(reqs))
     clocks = Clocks(0)
-    with kc.Server(ctx, streams=4, orientation="degen") as srv:
+    with kc.Server(ctx, streams=args.streams, orientation="degen") as srv:
         ids = [srv.put_graph(s, d, n) for s, d, n in resident]
         # warm-up: one request of each resident graph
         for gid in ids:
@@ -138,16 +149,14 @@ def run_serving(args):
             plain_counts.append(gr.count(k, mode="pivot", unit="node", part=0))
     t_plain = time.perf_counter() - t1
     exact = [r["count"] for r in results] == plain_counts
-    line = {"metric": "served graphs/s (Poisson %.0f req/s, R-MAT 1e3-%.0e edges, k 3-15)" % (args.rate, args.serve_max_edges),
+    return {"metric": "served graphs/s (Poisson %.0f req/s, R-MAT 1e3-%.0e edges, k 3-15)" % (args.rate, args.serve_max_edges),
             "value": served, "unit": "graphs/s", "n_gpus": 1, "higher_is_better": True,
             "p50_latency_ms": float(np.percentile(lat, 50)), "p99_latency_ms": float(np.percentile(lat, 99)),
             "plain": {"value": len(reqs) / t_plain, "unit": "graphs/s", "sample": "same requests, one per call"},
             "served_over_plain": served / (len(reqs) / t_plain), "bitexact": exact,
             "config": {"workload": "serving: %d requests, 30%% on 8 resident graphs, degeneracy orientation, "
-                                   "autotuned, 4 streams" % len(reqs)},
+                                   "autotuned, %d worker streams" % (len(reqs), args.streams)},
             "clocks": clk, "data": "synthetic (seeded generators)"}
-    print(json.dumps(line), flush=True)
-    ctx.close()
 
 
 def run_single(args):
@@ -483,6 +492,8 @@ def main():
             cpu = {"value": done / dt, "unit": UNIT, "cores": max_threads(), "kind": "port",
                    "sample": f"first {done} graphs of the batch, {dt:.1f} s, CPU oracle (OpenMP)",
                    "bitexact": bitexact_cpu}
+        # the serving configuration, bounded (a few seconds), on this GPU
+        serving = None if (args.no_serving or world > 1) else serving_leg(kc, ctx, args)
         h2d = 8 * E + 8 * (G + 1) + 8 * G
         ms_count = sum(stage["ms_count"]) / len(stage["ms_count"])
         ms_build = sum(stage["ms_build"]) / len(stage["ms_build"])
@@ -550,6 +561,7 @@ def main():
             "roofline": roofline,
             "roofline_issue": roofline_issue,
             "roofline_build": roofline_build,
+            "serving": serving,
             "host_ms": {"checks_h2d": host_ms[0], "build": host_ms[1], "plan": host_ms[2], "count": host_ms[3],
                         "readback": host_ms[4]},
         }

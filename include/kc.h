@@ -139,6 +139,13 @@ const char* kc_status_string(kc_status s);
  * share a method, each with this limit. The reference has no counterpart (its
  * count runs to completion, src/main.cu:303-580). */
 kc_status kc_ctx_set_time_limit(kc_ctx* ctx, uint64_t ns);
+/* Device memory the context keeps for reuse: the engine's temporaries and the
+ * arrays of destroyed graphs go back to a per-context cache of blocks, so
+ * repeated calls of the same sizes make no driver allocations (up to 16 GiB of
+ * free blocks are kept). This returns every cached block to the driver. No
+ * counterpart in the reference (it allocates and frees per call,
+ * kclique/kclique.cuh:1448-2623). */
+kc_status kc_ctx_release_cached_memory(kc_ctx* ctx);
 /* The CUDA stream (a cudaStream_t) every call of this context runs on, so a
  * caller can order its own work or record timing events on it. */
 kc_status kc_ctx_get_stream(kc_ctx* ctx, void** stream);

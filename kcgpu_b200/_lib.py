@@ -72,6 +72,7 @@ SIGNATURES = {
     "kc_last_error": (C.c_char_p, []),
     "kc_status_string": (C.c_char_p, [i32]),
     "kc_ctx_set_time_limit": (i32, [C.c_void_p, u64]),
+    "kc_ctx_release_cached_memory": (i32, [C.c_void_p]),
     "kc_ctx_get_stream": (i32, [C.c_void_p, P(C.c_void_p)]),
     "kc_kernel_launches": (u64, []),
     "kc_test_fail_alloc_after": (None, [i64]),

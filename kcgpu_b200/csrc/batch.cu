@@ -79,7 +79,7 @@ uint32_t grid_for(uint64_t work, int sms) {
 void free_union(kc_graph* g) {
   uint32_t** ps[] = {&g->rp, &g->col, &g->rank, &g->inv, &g->drp, &g->dcol, &g->erow, &g->prio, &g->level, &g->vgraph};
   for (uint32_t** p : ps) {
-    if (*p) cudaFreeAsync(*p, g->ctx->stream);
+    if (*p) dfree(*p, g->ctx->stream);
     *p = nullptr;
   }
 }

@@ -203,7 +203,7 @@ void count_release(CountPlan* pl) {
   for (int c = 0; c <= kNumClasses; ++c) release_launch(pl->launches[c], s);
   void* ps[] = {pl->cls, pl->ccnt, pl->queue, pl->scratch, pl->heavy};
   for (void* p : ps)
-    if (p) cudaFreeAsync(p, s);
+    if (p) dfree(p, s);
   pl->cls = nullptr;
   pl->ccnt = pl->queue = pl->scratch = pl->heavy = nullptr;
 }
@@ -251,11 +251,11 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
   if (req.mode != KC_MODE_ORIENT) KC_TRY(ensure_binom(ctx, pl->max_size + 2, k_max + 1));
   const uint32_t nu = std::max<uint32_t>(1, pl->n_units);
   pl->n_chunks = (nu + kPartChunk - 1) / kPartChunk;
-  KC_CUDA(cudaMallocAsync(&pl->cls, nu, s));
-  KC_CUDA(cudaMallocAsync(&pl->ccnt, sizeof(uint32_t) * ((size_t)kNumClasses * pl->n_chunks + 1), s));
-  KC_CUDA(cudaMallocAsync(&pl->queue, sizeof(uint32_t) * nu, s));
-  KC_CUDA(cudaMallocAsync(&pl->heavy, sizeof(uint32_t) * nu, s));
-  KC_CUDA(cudaMallocAsync(&pl->scratch, sizeof(uint32_t) * kScratchWords, s));
+  KC_CUDA(dmalloc(&pl->cls, nu, s));
+  KC_CUDA(dmalloc(&pl->ccnt, sizeof(uint32_t) * ((size_t)kNumClasses * pl->n_chunks + 1), s));
+  KC_CUDA(dmalloc(&pl->queue, sizeof(uint32_t) * nu, s));
+  KC_CUDA(dmalloc(&pl->heavy, sizeof(uint32_t) * nu, s));
+  KC_CUDA(dmalloc(&pl->scratch, sizeof(uint32_t) * kScratchWords, s));
   // Per-launch algorithm: orientation or pivot as requested; KC_MODE_AUTO
   // lists small units by orientation (cheap when their neighbourhood holds few
   // cliques) and counts large units and over-budget units with the pivot.

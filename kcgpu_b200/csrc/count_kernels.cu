@@ -1275,7 +1275,7 @@ kc_status prepare_launch(kc_ctx* ctx, const LaunchPlan& lp, const CountParams& p
     const uint64_t per_block = (uint64_t)gpb * p.gbuf_words * 4;
     const uint64_t cap = std::max<uint64_t>(1, (24ull << 30) / std::max<uint64_t>(1, per_block));
     grid = std::min(grid, cap);
-    KC_CUDA(cudaMallocAsync(&out->gbuf, grid * per_block, s));
+    KC_CUDA(dmalloc(&out->gbuf, grid * per_block, s));
     p.gbuf = out->gbuf;
   }
   out->p = p;
@@ -1297,7 +1297,7 @@ kc_status enqueue_launch(const PreparedLaunch& pl, cudaStream_t s) {
 }
 
 void release_launch(PreparedLaunch& pl, cudaStream_t s) {
-  if (pl.gbuf) cudaFreeAsync(pl.gbuf, s);
+  if (pl.gbuf) dfree(pl.gbuf, s);
   pl.gbuf = nullptr;
 }
 

@@ -555,7 +555,7 @@ kc_status prepare_launch_list(kc_ctx* ctx, const LaunchPlan& lp, const CountPara
   uint64_t grid = std::min<uint64_t>((uint64_t)ctx->sms * per_sm, ((uint64_t)p.n_units_max + gpb - 1) / gpb);
   const uint64_t per_block = (uint64_t)gpb * LY.total * 4;
   grid = std::max<uint64_t>(1, std::min<uint64_t>(grid, std::max<uint64_t>(1, (16ull << 30) / per_block)));
-  KC_CUDA(cudaMallocAsync(&out->gbuf, grid * per_block, s));
+  KC_CUDA(dmalloc(&out->gbuf, grid * per_block, s));
   p.gbuf = out->gbuf;
   out->p = p;
   out->grid = (uint32_t)grid;

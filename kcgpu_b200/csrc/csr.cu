@@ -32,23 +32,54 @@ __global__ void k_max_id(const uint32_t* __restrict__ src, const uint32_t* __res
   if (lane_id() == 0 && mx) atomicMax(out, mx);
 }
 
+// Edge lists usually arrive grouped by source (generators, sorted files), so
+// the lanes of a warp often share a source row: its counter is bumped once per
+// group of equal sources (__match_any_sync), not once per lane. Whole warps
+// walk the grid-stride loop together; lanes past the end or on a self-loop
+// carry the key 0xffffffff and do nothing.
+__device__ __forceinline__ uint32_t grouped_add(uint32_t* ctr, uint32_t key, uint32_t lane) {
+  const uint32_t peers = __match_any_sync(0xffffffffu, key);
+  const uint32_t leader = (uint32_t)__ffs(peers) - 1u;
+  uint32_t base = 0;
+  if (lane == leader && key != 0xffffffffu) base = atomicAdd(&ctr[key], (uint32_t)__popc(peers));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  return base + (uint32_t)__popc(peers & lanemask_lt());
+}
+
 __global__ void k_degree(const uint32_t* __restrict__ src, const uint32_t* __restrict__ dst, uint64_t E,
                          uint32_t* deg) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < E; i += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t u = src[i], v = dst[i];
-    if (u == v) continue;
-    atomicAdd(&deg[u], 1u);
-    atomicAdd(&deg[v], 1u);
+  const uint32_t lane = lane_id();
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); b < E; b += stride) {
+    const uint64_t i = b + lane;
+    uint32_t u = 0xffffffffu, v = 0xffffffffu;
+    if (i < E) {
+      u = src[i];
+      v = dst[i];
+      if (u == v) u = v = 0xffffffffu;
+    }
+    grouped_add(deg, u, lane);
+    if (v != 0xffffffffu) atomicAdd(&deg[v], 1u);
   }
 }
 
 __global__ void k_scatter(const uint32_t* __restrict__ src, const uint32_t* __restrict__ dst, uint64_t E,
                           uint32_t* cursor, uint32_t* adj) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < E; i += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t u = src[i], v = dst[i];
-    if (u == v) continue;
-    adj[atomicAdd(&cursor[u], 1u)] = v;
-    adj[atomicAdd(&cursor[v], 1u)] = u;
+  const uint32_t lane = lane_id();
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); b < E; b += stride) {
+    const uint64_t i = b + lane;
+    uint32_t u = 0xffffffffu, v = 0xffffffffu;
+    if (i < E) {
+      u = src[i];
+      v = dst[i];
+      if (u == v) u = v = 0xffffffffu;
+    }
+    const uint32_t pu = grouped_add(cursor, u, lane);
+    if (u != 0xffffffffu) {
+      adj[pu] = v;
+      adj[atomicAdd(&cursor[v], 1u)] = u;
+    }
   }
 }
 

@@ -15,6 +15,7 @@
 #include <string>
 #include <vector>
 
+#include "count_kernels.cuh"
 #include "dev_common.cuh"
 #include "engine.h"
 #include "prims.cuh"
@@ -23,14 +24,14 @@ namespace kc {
 
 kc_status dev_alloc(kc_graph* g, void** p, size_t bytes) {
   bytes = std::max<size_t>(bytes, 4);
-  cudaError_t e = cudaMallocAsync(p, bytes, g->ctx->stream);
+  cudaError_t e = dmalloc_raw(p, bytes, g->ctx->stream);
   if (e != cudaSuccess) return cuda_fail(e, "device allocation", __FILE__, __LINE__);
   g->bytes += bytes;
   return KC_OK;
 }
 
 void dev_free(kc_graph* g, void* p) {
-  if (p) cudaFreeAsync(p, g->ctx->stream);
+  if (p) dfree(p, g->ctx->stream);
 }
 
 namespace {
@@ -55,7 +56,7 @@ struct CtxLock {
 void free_graph_arrays(kc_graph* g) {
   void* ps[] = {g->rp, g->col, g->rank, g->inv, g->drp, g->dcol, g->erow, g->prio, g->level, g->vgraph};
   for (void* p : ps)
-    if (p) cudaFreeAsync(p, g->ctx->stream);
+    if (p) dfree(p, g->ctx->stream);
   g->rp = g->col = g->rank = g->inv = g->drp = g->dcol = g->erow = g->prio = g->level = g->vgraph = nullptr;
 }
 
@@ -81,9 +82,11 @@ kc_params autotune(uint32_t n, uint64_t m, uint32_t max_out, uint32_t k, uint32_
   // Per-graph choice from shape features.
   //  * mode: pivoting wins when the graph holds large cliques (its cost follows
   //    the clique tree, not the clique count); orientation listing wins on
-  //    sparse neighbourhoods. Graphs whose peel shows a dense core pivot
-  //    outright; the others run KC_MODE_AUTO, which lists small units and moves
-  //    any unit that outgrows its budget (a hidden clique) to the pivot.
+  //    sparse neighbourhoods. A unit inside a c-core lists about C(c, k - 1)
+  //    cliques, so a graph whose core would make that a sizeable part of a
+  //    warp unit's work budget (kUnitBudget / 4) pivots outright; the others
+  //    run KC_MODE_AUTO, which lists small units and moves any unit that
+  //    outgrows its budget (a hidden clique) to the pivot.
   //  * part: 0 lets each size class size its partitions to its word width.
   //  * unit: edge units spread the work of graphs with few vertices but wide
   //    out-neighbourhoods over more groups.
@@ -92,7 +95,10 @@ kc_params autotune(uint32_t n, uint64_t m, uint32_t max_out, uint32_t k, uint32_
   std::memset(&p, 0, sizeof(p));
   p.k = k;
   const double dens = n > 1 ? (2.0 * (double)m) / ((double)n * (n - 1)) : 0.0;
-  const bool dense_core = max_core >= 24 || (max_core + 1 >= k && k >= 7 && max_core >= 12);
+  double listed = 1.0;  // C(max_core, k - 1)
+  for (uint32_t i = 0; k >= 1 && i < k - 1 && i < max_core; ++i) listed = listed * (max_core - i) / (i + 1);
+  if (k >= 1 && k - 1 > max_core) listed = 0.0;
+  const bool dense_core = max_core >= 24 || listed > kUnitBudget / 4.0;
   p.mode = dense_core ? KC_MODE_PIVOT : KC_MODE_AUTO;
   p.unit = (n < 256 && max_out > 64) ? KC_UNIT_EDGE : KC_UNIT_NODE;
   p.part = 0;
@@ -151,13 +157,23 @@ kc_status kc_ctx_create(int device, kc_ctx** out) {
   c->max_smem_optin = (int)prop.sharedMemPerBlockOptin;
   c->total_mem = prop.totalGlobalMem;
   KC_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-  // keep freed stream-ordered memory in the pool between calls
+  // keep freed stream-ordered memory in the pool between calls, and reuse the
+  // context's own blocks before asking the pool (devmem.cpp)
   cudaMemPool_t pool;
   if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
     uint64_t thr = UINT64_MAX;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
   }
+  kc::register_stream_cache(c->stream, &c->cache);
   *out = c;
+  return KC_OK;
+}
+
+kc_status kc_ctx_release_cached_memory(kc_ctx* ctx) {
+  if (!ctx) return fail(KC_ERR_INVALID_ARG, "context is NULL");
+  kc::CtxLock lock(ctx);
+  ctx->cache.release(ctx->stream);
+  KC_CUDA(cudaStreamSynchronize(ctx->stream));
   return KC_OK;
 }
 
@@ -178,6 +194,9 @@ kc_status kc_ctx_destroy(kc_ctx* ctx) {
       if (ctx->tend[c]) cudaEventDestroy(ctx->tend[c]);
     }
     if (ctx->fork) cudaEventDestroy(ctx->fork);
+    ctx->cache.release(ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    kc::unregister_stream_cache(ctx->stream);
     cudaStreamDestroy(ctx->stream);
   }
   delete ctx;

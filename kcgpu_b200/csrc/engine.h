@@ -16,6 +16,7 @@ struct kc_ctx {
   int sms = 148;
   int max_smem_optin = 227 * 1024;
   uint64_t time_limit_ns = 0;  // device time limit of a counting pass (0 = none)
+  kc::BlockCache cache;        // device blocks reused by allocations on `stream`
   uint64_t total_mem = 0;
   std::mutex mu;  // one call at a time per context
   // exact binomial table C(r, c) as (lo, hi) pairs, rows [0, brows], cols [0, bcols]

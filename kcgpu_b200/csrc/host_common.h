@@ -6,7 +6,10 @@
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -32,14 +35,47 @@ inline double now_ms() {
   return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
 }
 
-// Device temporaries of one call: allocated stream-ordered on s and freed,
-// stream-ordered, when the guard goes out of scope, so a call that fails half
-// way leaks nothing. free_now() hands one back early to lower the peak.
+// Per-context cache of device blocks (devmem.cpp): blocks freed on the
+// context's stream are reused by later allocations on that stream.
+class BlockCache {
+ public:
+  cudaError_t get(void** p, size_t bytes, cudaStream_t s);
+  void put(void* p, cudaStream_t s);
+  void release(cudaStream_t s);  // returns every free block to the driver
+  uint64_t cached_bytes();
+
+ private:
+  std::mutex mu_;
+  std::multimap<size_t, void*> free_;
+  std::unordered_map<void*, size_t> size_;  // every block of this cache, free or in use
+  uint64_t free_bytes_ = 0;
+};
+
+// The cache serving allocations on stream s (a context's stream).
+void register_stream_cache(cudaStream_t s, BlockCache* c);
+void unregister_stream_cache(cudaStream_t s);
+
+// Every device allocation of the engine: from the cache registered for s,
+// else straight from the stream-ordered allocator; dfree returns the block
+// the same way (stream-ordered on s).
+cudaError_t dmalloc_raw(void** p, size_t bytes, cudaStream_t s);
+template <class T>
+cudaError_t dmalloc(T** p, size_t bytes, cudaStream_t s) {
+  void* q = nullptr;
+  const cudaError_t e = dmalloc_raw(&q, bytes, s);
+  *p = static_cast<T*>(q);
+  return e;
+}
+void dfree(void* p, cudaStream_t s);
+
+// Device temporaries of one call: allocated on s and freed, stream-ordered,
+// when the guard goes out of scope, so a call that fails half way leaks
+// nothing. free_now() hands one back early to lower the peak.
 class DevTemps {
  public:
   explicit DevTemps(cudaStream_t s) : s_(s) {}
   ~DevTemps() {
-    for (void* p : ps_) cudaFreeAsync(p, s_);
+    for (void* p : ps_) dfree(p, s_);
   }
   DevTemps(const DevTemps&) = delete;
   DevTemps& operator=(const DevTemps&) = delete;
@@ -47,7 +83,7 @@ class DevTemps {
   template <class T>
   cudaError_t alloc(T** p, size_t bytes) {
     void* q = nullptr;
-    const cudaError_t e = cudaMallocAsync(&q, bytes ? bytes : 4, s_);
+    const cudaError_t e = dmalloc_raw(&q, bytes, s_);
     *p = static_cast<T*>(q);
     if (e == cudaSuccess) ps_.push_back(q);
     return e;
@@ -56,7 +92,7 @@ class DevTemps {
   void free_now(void* p) {
     for (size_t i = 0; i < ps_.size(); ++i)
       if (ps_[i] == p) {
-        cudaFreeAsync(p, s_);
+        dfree(p, s_);
         ps_.erase(ps_.begin() + (long)i);
         return;
       }

@@ -7,6 +7,7 @@
 #include <cstdio>
 
 #include "dev_common.cuh"
+#include "host_common.h"
 #include "prims.cuh"
 
 namespace kc {
@@ -120,15 +121,15 @@ template <class TO>
 cudaError_t scan_impl(const uint32_t* in, TO* out, size_t n, cudaStream_t s) {
   const uint32_t nb = (uint32_t)std::max<size_t>(1, (n + TILE - 1) / TILE);
   TO* sums = nullptr;
-  cudaError_t e = cudaMallocAsync(&sums, sizeof(TO) * nb, s);
+  cudaError_t e = kc::dmalloc(&sums, sizeof(TO) * nb, s);
   if (e != cudaSuccess) return e;
   if (n) k_scan_reduce<TO><<<nb, NT, 0, s>>>(in, n, sums);
   else e = cudaMemsetAsync(sums, 0, sizeof(TO) * nb, s);
-  if (e != cudaSuccess) { cudaFreeAsync(sums, s); return e; }
+  if (e != cudaSuccess) { kc::dfree(sums, s); return e; }
   k_scan_sums<TO><<<1, NT, 0, s>>>(sums, nb, out + n);
   if (n) k_scan_apply<TO><<<nb, NT, 0, s>>>(in, out, n, sums);
   e = cudaGetLastError();
-  cudaFreeAsync(sums, s);
+  kc::dfree(sums, s);
   return e;
 }
 
@@ -466,7 +467,7 @@ cudaError_t radix_sort_u64(unsigned long long* keys, unsigned long long* tmp, si
   if (n <= 1 || bits <= 0) return cudaSuccess;
   const uint32_t nb = (uint32_t)((n + TILE - 1) / TILE);
   uint32_t* hist = nullptr;
-  cudaError_t e = cudaMallocAsync(&hist, sizeof(uint32_t) * ((size_t)256 * nb + 1), s);
+  cudaError_t e = kc::dmalloc(&hist, sizeof(uint32_t) * ((size_t)256 * nb + 1), s);
   if (e != cudaSuccess) return e;
   unsigned long long* a = keys;
   unsigned long long* b = tmp;
@@ -480,7 +481,7 @@ cudaError_t radix_sort_u64(unsigned long long* keys, unsigned long long* tmp, si
   }
   if (e == cudaSuccess && (passes & 1))
     e = cudaMemcpyAsync(keys, a, n * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, s);
-  cudaFreeAsync(hist, s);
+  kc::dfree(hist, s);
   if (e == cudaSuccess) e = cudaGetLastError();
   return e;
 }
@@ -491,15 +492,15 @@ cudaError_t segmented_sort_unique(const uint32_t* off, uint32_t* data, uint32_t*
   uint32_t* lists = nullptr;
   uint32_t* counts = nullptr;
   unsigned long long* huge_total = nullptr;
-  cudaError_t e = cudaMallocAsync(&lists, sizeof(uint32_t) * (size_t)RC_N * n_rows, s);
+  cudaError_t e = kc::dmalloc(&lists, sizeof(uint32_t) * (size_t)RC_N * n_rows, s);
   if (e != cudaSuccess) return e;
   // 8 class counters (RC_N used) followed by the 64-bit total of the huge rows
   constexpr size_t kCountBytes = sizeof(uint32_t) * 8 + sizeof(unsigned long long) * 2;
-  e = cudaMallocAsync(&counts, kCountBytes, s);
-  if (e != cudaSuccess) { cudaFreeAsync(lists, s); return e; }
+  e = kc::dmalloc(&counts, kCountBytes, s);
+  if (e != cudaSuccess) { kc::dfree(lists, s); return e; }
   huge_total = reinterpret_cast<unsigned long long*>(counts + 8);
   e = cudaMemsetAsync(counts, 0, kCountBytes, s);
-  if (e != cudaSuccess) { cudaFreeAsync(lists, s); cudaFreeAsync(counts, s); return e; }
+  if (e != cudaSuccess) { kc::dfree(lists, s); kc::dfree(counts, s); return e; }
   const int sms = num_sms();
   {
     uint32_t grid = (uint32_t)std::min<size_t>((n_rows + 255) / 256, (size_t)sms * 16);
@@ -537,12 +538,12 @@ cudaError_t segmented_sort_unique(const uint32_t* off, uint32_t* data, uint32_t*
       uint32_t *hlen = nullptr, *hstart = nullptr, *flag = nullptr, *pos = nullptr;
       unsigned long long *keys = nullptr, *tmp = nullptr;
       // every allocation is checked: a failed one must stop the sort before a kernel sees its null pointer
-      e = cudaMallocAsync(&hlen, sizeof(uint32_t) * (H + 1), s);
-      if (e == cudaSuccess) e = cudaMallocAsync(&hstart, sizeof(uint32_t) * (H + 1), s);
-      if (e == cudaSuccess) e = cudaMallocAsync(&keys, sizeof(unsigned long long) * T, s);
-      if (e == cudaSuccess) e = cudaMallocAsync(&tmp, sizeof(unsigned long long) * T, s);
-      if (e == cudaSuccess) e = cudaMallocAsync(&flag, sizeof(uint32_t) * T, s);
-      if (e == cudaSuccess) e = cudaMallocAsync(&pos, sizeof(uint32_t) * (T + 1), s);
+      e = kc::dmalloc(&hlen, sizeof(uint32_t) * (H + 1), s);
+      if (e == cudaSuccess) e = kc::dmalloc(&hstart, sizeof(uint32_t) * (H + 1), s);
+      if (e == cudaSuccess) e = kc::dmalloc(&keys, sizeof(unsigned long long) * T, s);
+      if (e == cudaSuccess) e = kc::dmalloc(&tmp, sizeof(unsigned long long) * T, s);
+      if (e == cudaSuccess) e = kc::dmalloc(&flag, sizeof(uint32_t) * T, s);
+      if (e == cudaSuccess) e = kc::dmalloc(&pos, sizeof(uint32_t) * (T + 1), s);
       if (e == cudaSuccess) {
         k_huge_lengths<<<(H + 255) / 256, 256, 0, s>>>(off, hlist, H, hlen);
         e = scan_exclusive_u32(hlen, hstart, H, s);
@@ -559,11 +560,11 @@ cudaError_t segmented_sort_unique(const uint32_t* off, uint32_t* data, uint32_t*
       }
       void* hp[] = {hlen, hstart, keys, tmp, flag, pos};
       for (void* p : hp)
-        if (p) cudaFreeAsync(p, s);
+        if (p) kc::dfree(p, s);
     }
   }
-  cudaFreeAsync(lists, s);
-  cudaFreeAsync(counts, s);
+  kc::dfree(lists, s);
+  kc::dfree(counts, s);
   return e;
 }
 

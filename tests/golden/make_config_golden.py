@@ -94,17 +94,20 @@ def run_graph(fx: dict, name: str, budget: float) -> None:
     rec["m"] = og.m
     rec["max_out_degree"] = og.orient(orient)
     spent = 0.0
-    last = 0.0
+    last, prev = 0.0, 0.0
     for k in ks:
         if str(k) in rec["counts"]:
+            prev, last = last, float(rec["oracle_seconds"].get(str(k), 0.0))
             continue
-        # the cost grows with k; stop when the next count would not fit
-        if last and spent + 30 * last > budget:
+        # the cost grows with k: predict the next count from the growth of the
+        # last two and stop when it would not fit the budget
+        growth = max(2.0, last / prev) if prev > 0 else 4.0
+        if last and spent + growth * last > budget:
             rec.setdefault("not_counted", []).append(k)
             continue
         t0 = time.perf_counter()
         c = og.count(k, mode, "node", closed=(mode == "pivot"))
-        last = time.perf_counter() - t0
+        prev, last = last, time.perf_counter() - t0
         spent += last
         rec["counts"][str(k)] = str(c)
         rec["oracle_seconds"][str(k)] = round(last, 2)
