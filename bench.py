@@ -37,10 +37,17 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "graphs/s, batched exact k-clique counts (10,000 mixed small graphs, k 4-12)"
 UNIT = "graphs/s"
-# DRAM bytes (read + write) of one step's counting launches, from the ncu
-# capture summarised in the file named below; None until captured.
-COUNT_DRAM_BYTES_PER_STEP = None
-COUNT_DRAM_SOURCE = None
+# DRAM bytes (read + write) per input edge of one step's counting launches and
+# of its build (CSR, orientation, queue) launches, from the ncu capture of the
+# first 1,500 graphs of the batch (53,548,148 input edges) summarised in the
+# file named below; a step's traffic is scaled from it by its input edges
+# (both grow with the edges: the gather with the out-lists, the build with the
+# pairs it reads and the CSR it writes).
+DRAM_CAPTURE_EDGES = 53_548_148
+COUNT_DRAM_BYTES_CAPTURED = 298.2e6 + 1.7e6
+BUILD_DRAM_BYTES_CAPTURED = 6.21e9
+DRAM_SOURCE = ("profiles/build_kernels_batched1500_dram.md (ncu dram__bytes_read.sum + dram__bytes_write.sum, "
+               "1,500-graph capture scaled by input edges)")
 
 
 def parse():
@@ -59,11 +66,17 @@ def parse():
     ap.add_argument("--ks", default="", help="single-graph legs: comma-separated k values")
     ap.add_argument("--unit", default="", help="single-graph legs: node|edge (default: the config's)")
     ap.add_argument("--part", type=int, default=-1, help="single-graph legs: partition size (default: the config's)")
+    ap.add_argument("--time-limit", type=float, default=900.0,
+                    help="single-graph legs: device time limit of one count in seconds (the count then reports "
+                         "a timeout instead of a number)")
     ap.add_argument("--requests", type=int, default=128)
     ap.add_argument("--rate", type=float, default=2000.0)
     ap.add_argument("--serve-max-edges", type=float, default=1e5)
     ap.add_argument("--streams", type=int, default=8, help="serving: worker contexts / streams")
     ap.add_argument("--no-serving", action="store_true", help="batched workload: skip the serving leg")
+    ap.add_argument("--tune-sample", type=int, default=1500, help="batched: graphs of the autotuner comparison")
+    ap.add_argument("--tune-time-limit", type=float, default=5.0,
+                    help="batched: device seconds per counting pass in the autotuner comparison")
     return ap.parse_args()
 
 
@@ -89,6 +102,61 @@ def serving_requests(kc, n_req: int, seed: int, max_edges: float = 1e5):
             scale = max(1, int(np.ceil(np.log2(E / 16))))
             reqs.append(("oneshot", kc.gen_rmat(scale, E / (1 << scale), seed=seed * 1000 + 100 + r).arrays(), k))
     return resident, reqs
+
+
+def spec_label(c: dict) -> str:
+    """The reference's -q spelling of a method plus the unit ("p8b-node");
+    partition 0 (each size class sizes its own) prints as A."""
+    return "%s%s%s-%s" % ("opa"[c["mode"]], c["part"] if c["part"] else "A", "bn"[c["encoding"]],
+                          ("node", "edge")[c["unit"]])
+
+
+def autotune_leg(kc, ctx, s, d, off, nn, kk, choice, args):
+    """The autotuner's choices on the batch (histogram), and the counting stage
+    of a bounded sample of the batch (its first graphs) under the autotuner and
+    under fixed methods: the sweep's best fixed method and the reference's
+    two partition-8 bitmap methods. Device ms of the counting stage from the
+    batch statistics; a method past the device time limit reports null."""
+    from collections import Counter
+
+    hist = Counter(spec_label(c) for c in choice)
+    P = min(len(nn), args.tune_sample)
+    a, b = 0, int(off[P])
+    ss, dd, oo = s[a:b], d[a:b], off[:P + 1]
+    sweep = {}
+    try:
+        sweep = json.loads((ROOT / "kcgpu_b200" / "autotune_sweep.json").read_text())
+    except (OSError, ValueError):
+        pass
+    fixed = {"o8b-node": {"mode": "orient", "unit": "node", "part": 8, "encoding": "bitmap"},
+             "p8b-node": {"mode": "pivot", "unit": "node", "part": 8, "encoding": "bitmap"}}
+    bf = sweep.get("best_fixed_method")
+    if bf:
+        code, unit = bf.split("-")
+        fixed[bf] = {"mode": {"o": "orient", "p": "pivot", "a": "auto"}[code[0]], "unit": unit,
+                     "part": 0 if code[1:-1] == "A" else int(code[1:-1]),
+                     "encoding": "bitmap" if code[-1] == "b" else "list"}
+    runs = {}
+    ctx.set_time_limit(int(args.tune_time_limit * 1e9))
+    try:
+        for name, fx in [("autotuned", None)] + list(fixed.items()):
+            try:
+                best = None
+                for _ in range(2):
+                    _, st = kc.batch_count(ctx, ss, dd, oo, nn[:P], kk[:P], orientation="degree",
+                                           autotune=fx is None, fixed=fx, return_stats=True)
+                    best = st["ms_count"] if best is None else min(best, st["ms_count"])
+                runs[name] = {"ms_count": best, "graphs_per_s_count_stage": P / (best / 1e3)}
+            except kc.KCError as e:
+                if e.name != "KC_ERR_DEVICE_TIMEOUT":
+                    raise
+                runs[name] = {"ms_count": None, "timeout_s": args.tune_time_limit}
+    finally:
+        ctx.set_time_limit(0)
+    done = [v["ms_count"] for k, v in runs.items() if k != "autotuned" and v["ms_count"] is not None]
+    return {"choice_histogram": dict(hist.most_common()), "sample": f"first {P} graphs of the batch",
+            "counting_stage": runs, "sweep_best_fixed": bf,
+            "tuned_over_best_fixed": (min(done) / runs["autotuned"]["ms_count"]) if done else None}
 
 
 def run_serving(args):
@@ -170,13 +238,19 @@ def run_single(args):
                 pivoting, edge units, partition 8, bitmap, k = 5, 7
       chunglu : Chung-Lu n = 4M, exponent 2.1, mean degree 20, cap 50k, 200
                 planted cliques of 30-60, degeneracy, pivoting, node units,
-                k = 3, 6, 9, 12"""
+                k = 3, 6, 9, 12
+    Under torchrun (N > 1) every rank builds the whole graph and counts one
+    unit shard of it (kc_count_shard); the counts are summed exactly over the
+    ranks and the device time is the max over ranks (strong scaling)."""
     import torch
 
     import kcgpu_b200 as kc
+    from kcgpu_b200 import sharding
 
-    torch.cuda.set_device(0)
-    ctx = kc.Context(0)
+    world, rank, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    ctx = kc.Context(local)
+    shard = (rank, world) if world > 1 else None
     if args.workload == "er":
         el = kc.gen_er(2000, 0.01, 1)
         orient, mode, unit, part, ks, enc = "degree", "orient", "node", 8, [4], "bitmap"
@@ -197,30 +271,69 @@ def run_single(args):
     if args.part >= 0:
         part = args.part
     s, d, n = el.arrays()
-    clocks = Clocks(0)
+    # exact counts of the same graph from the CPU oracle, when the fixture
+    # file holds them (matched by the sha256 of the generated arrays)
+    want = {}
+    try:
+        import hashlib
+
+        h = hashlib.sha256()
+        h.update(np.ascontiguousarray(s).tobytes())
+        h.update(np.ascontiguousarray(d).tobytes())
+        fx = json.loads((ROOT / "tests" / "golden" / "configs.json").read_text())["configs"]
+        for rec in fx.values():
+            if rec.get("input_sha256") == h.hexdigest() and isinstance(rec.get("counts"), dict):
+                want = {int(k): int(v) for k, v in rec["counts"].items()}
+    except (OSError, ValueError, KeyError):
+        pass
+    clocks = Clocks(local)
     with kc.Graph.from_edges(ctx, s, d, n) as g:
         g.orient(orient)
         info = g.info()
         rows = []
         g.count(3, mode=mode, unit=unit, part=part, encoding=enc)  # warm-up: loads and sizes every kernel
+        ctx.set_time_limit(int(args.time_limit * 1e9))
         for k in ks:
+            barrier(pg, local)
             clocks.start()
             t0 = time.perf_counter()
-            r = g.count(k, mode=mode, unit=unit, part=part, encoding=enc, stats=True)
+            try:
+                r = g.count(k, mode=mode, unit=unit, part=part, encoding=enc, stats=True, shard=shard)
+                ok = 1.0
+            except kc.KCError as e:
+                if e.name != "KC_ERR_DEVICE_TIMEOUT":
+                    raise
+                r, ok = None, 0.0
+            # every rank takes the same collective steps, timeout or not
+            ok = -max_over_ranks(pg, -ok, local)
+            if not ok:
+                clk = clocks.stop()
+                clocks = Clocks(local)
+                rows.append({"k": k, "count": None, "timeout_s": args.time_limit,
+                             "wall_ms": (time.perf_counter() - t0) * 1e3, "clocks": clk})
+                continue
             wall = time.perf_counter() - t0
             clk = clocks.stop()
-            clocks = Clocks(0)
-            ms = r.stats["ms_total"]
-            rows.append({"k": k, "count": str(r.count), "ms": ms, "wall_ms": wall * 1e3,
-                         "kcliques_per_s": r.count / (ms / 1e3) if ms > 0 else None,
-                         "tree_nodes": r.stats["tree_nodes"], "ms_launch": r.stats["ms_launch"],
-                         "clocks": clk})
+            clocks = Clocks(local)
+            ms = max_over_ranks(pg, r.stats["ms_total"], local)
+            count = sharding.sum_u128(r.count) if pg is not None else r.count
+            tree = int(max_over_ranks(pg, float(r.stats["tree_nodes"]), local))
+            rows.append({"k": k, "count": str(count), "ms": ms, "wall_ms": wall * 1e3,
+                         "kcliques_per_s": count / (ms / 1e3) if ms > 0 else None,
+                         "tree_nodes" if pg is None else "tree_nodes_max_rank": tree,
+                         "ms_launch": r.stats["ms_launch"],
+                         "oracle_fixture": (count == want[k]) if k in want else None, "clocks": clk})
     line = {"metric": "single-graph k-clique counts (device ms per count)", "workload": args.workload,
+            "n_gpus": world, "scaling": "strong" if world > 1 else None,
             "config": {"workload": name, "n": info["n"], "m": info["m"], "max_out_degree": info["max_out_degree"],
-                       "orientation": orient, "mode": mode, "unit": unit, "part": part, "encoding": enc},
+                       "orientation": orient, "mode": mode, "unit": unit, "part": part, "encoding": enc,
+                       "parallelism": "unit shards over %d GPUs" % world if world > 1 else "single GPU"},
             "results": rows, "data": "synthetic (seeded generators)"}
-    print(json.dumps(line), flush=True)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     ctx.close()
+    if pg is not None:
+        pg.destroy_process_group()
 
 
 class Clocks:
@@ -494,6 +607,7 @@ def main():
                    "bitexact": bitexact_cpu}
         # the serving configuration, bounded (a few seconds), on this GPU
         serving = None if (args.no_serving or world > 1) else serving_leg(kc, ctx, args)
+        tuning = autotune_leg(kc, ctx, s, d, off, nn, kk, choice, args)
         h2d = 8 * E + 8 * (G + 1) + 8 * G
         ms_count = sum(stage["ms_count"]) / len(stage["ms_count"])
         ms_build = sum(stage["ms_build"]) / len(stage["ms_build"])
@@ -518,8 +632,8 @@ def main():
         roofline = {"bound": "hbm", "kernel": "k_count_bitmap (all counting launches of a step)",
                     "achieved": gb_s, "peak": hbm_peak, "unit": "GB/s", "frac": gb_s / hbm_peak,
                     "peak_source": peak_src, "algorithmic_bytes_per_step": trav["gather_bytes"] / steps,
-                    "traffic": COUNT_DRAM_BYTES_PER_STEP,
-                    "traffic_source": COUNT_DRAM_SOURCE,
+                    "traffic": COUNT_DRAM_BYTES_CAPTURED * E / DRAM_CAPTURE_EDGES,
+                    "traffic_source": DRAM_SOURCE,
                     "limiter": "not HBM: latency and integer issue of the gather and traversal (roofline_issue)"}
         # The same launch against its real limiter: where its unit groups spend
         # their cycles, and its AND+POPC word-operation rate against the POPC
@@ -539,6 +653,7 @@ def main():
                           "achieved": build_bytes / (ms_build / 1e3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
                           "frac": build_bytes / (ms_build / 1e3) / 1e9 / hbm_peak, "peak_source": peak_src,
                           "algorithmic_bytes_per_step": build_bytes,
+                          "traffic": BUILD_DRAM_BYTES_CAPTURED * E / DRAM_CAPTURE_EDGES, "traffic_source": DRAM_SOURCE,
                           "ms": {"csr": sum(stage["ms_csr"]) / steps, "orient": sum(stage["ms_orient"]) / steps}}
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -562,6 +677,7 @@ def main():
             "roofline_issue": roofline_issue,
             "roofline_build": roofline_build,
             "serving": serving,
+            "autotune": tuning,
             "host_ms": {"checks_h2d": host_ms[0], "build": host_ms[1], "plan": host_ms[2], "count": host_ms[3],
                         "readback": host_ms[4]},
         }

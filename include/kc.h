@@ -139,6 +139,15 @@ const char* kc_status_string(kc_status s);
  * share a method, each with this limit. The reference has no counterpart (its
  * count runs to completion, src/main.cu:303-580). */
 kc_status kc_ctx_set_time_limit(kc_ctx* ctx, uint64_t ns);
+/* Host-input batches (kc_batch_count, kc_batch_count_packed) holding more
+ * than `edges` edges are counted as a pipeline of chunks of whole graphs of
+ * about `edges` edges each: while one chunk is built and counted, the next
+ * chunk's edges are copied to the device on a second stream, so the
+ * host->device copy of all but the first chunk is hidden behind device work.
+ * Counts and choices are the same as in one pass; kc_batch_stats add up the
+ * chunks (ms_h2d is the copy stream's time). 0 = the default (48M edges),
+ * UINT64_MAX = never split. Device-input batches always run in one pass. */
+kc_status kc_ctx_set_batch_chunk_edges(kc_ctx* ctx, uint64_t edges);
 /* Device memory the context keeps for reuse: the engine's temporaries and the
  * arrays of destroyed graphs go back to a per-context cache of blocks, so
  * repeated calls of the same sizes make no driver allocations (up to 16 GiB of
@@ -190,6 +199,18 @@ kc_status kc_graph_get_peel(const kc_graph* g, uint32_t* priority, uint32_t* lev
 
 /* ---- counting -------------------------------------------------------- */
 kc_status kc_count(kc_graph* g, const kc_params* p, kc_u128* out, kc_count_stats* stats);
+/* One unit shard of kc_count, for counting one graph on several GPUs (each
+ * process holds the whole graph and counts its shard; the caller adds the
+ * shards' counts, e.g. with an all-gather of the 16-byte results). Units are
+ * the node or edge units of kc_count, dealt out by position inside their size
+ * class: unit j of a class goes to shard j mod n_shards, so neighbouring units
+ * and the few largest ones are spread evenly. The counts of shards
+ * 0..n_shards-1 add up to kc_count's for the same graph and parameters
+ * (k <= 2 counts belong to shard 0). stats describe this shard's units. No
+ * reference counterpart (the reference counts on one GPU; its unit windows
+ * are kclique/kclique.cuh:1645-1675). */
+kc_status kc_count_shard(kc_graph* g, const kc_params* p, uint32_t shard, uint32_t n_shards, kc_u128* out,
+                         kc_count_stats* stats);
 /* Local (per-vertex) counts, the reference's -m lkc: per_vertex[v] = number of
  * k-cliques that contain vertex v (host array of n, indexed by vertex id);
  * total (may be NULL) = the k-clique count. Binary encoding (list encoding is

@@ -70,6 +70,12 @@ class Context:
         a pass past it raises KCError KC_ERR_DEVICE_TIMEOUT."""
         check(lib().kc_ctx_set_time_limit(self._h, int(ns)))
 
+    def set_batch_chunk_edges(self, edges: int) -> None:
+        """Host-input batches with more edges than this are counted as a
+        pipeline of chunks of whole graphs, the next chunk's copy overlapping
+        the current chunk's work (0 = the default, 2**64 - 1 = never)."""
+        check(lib().kc_ctx_set_batch_chunk_edges(self._h, int(edges)))
+
     def close(self):
         if self._h:
             lib().kc_ctx_destroy(self._h)
@@ -188,8 +194,10 @@ class Graph:
         return prio[:n], lev[:n]
 
     def count(self, k: int, mode="orient", unit="node", part: int = 8, encoding="bitmap",
-              stats: bool = False):
-        """Exact number of k-cliques (a Python int; 128-bit on the device)."""
+              stats: bool = False, shard: tuple[int, int] | None = None):
+        """Exact number of k-cliques (a Python int; 128-bit on the device).
+        shard=(i, S): only unit shard i of S (kc_count_shard); the S shards'
+        counts add up to the whole count."""
         p = KcParams()
         p.k = k
         p.mode = MODES[mode] if isinstance(mode, str) else int(mode)
@@ -199,7 +207,11 @@ class Graph:
         p.flags = 1 if stats else 0
         out = KcU128()
         st = KcCountStats()
-        check(lib().kc_count(self._h, C.byref(p), C.byref(out), C.byref(st)))
+        if shard is None:
+            check(lib().kc_count(self._h, C.byref(p), C.byref(out), C.byref(st)))
+        else:
+            check(lib().kc_count_shard(self._h, C.byref(p), int(shard[0]), int(shard[1]), C.byref(out),
+                                       C.byref(st)))
         if stats:
             vals = {f: getattr(st, f) for f, _ in KcCountStats._fields_ if f != "reserved"}
             vals["ms_launch"] = list(vals["ms_launch"])

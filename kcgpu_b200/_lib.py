@@ -72,6 +72,7 @@ SIGNATURES = {
     "kc_last_error": (C.c_char_p, []),
     "kc_status_string": (C.c_char_p, [i32]),
     "kc_ctx_set_time_limit": (i32, [C.c_void_p, u64]),
+    "kc_ctx_set_batch_chunk_edges": (i32, [C.c_void_p, u64]),
     "kc_ctx_release_cached_memory": (i32, [C.c_void_p]),
     "kc_ctx_get_stream": (i32, [C.c_void_p, P(C.c_void_p)]),
     "kc_kernel_launches": (u64, []),
@@ -87,6 +88,7 @@ SIGNATURES = {
     "kc_graph_get_dag": (i32, [C.c_void_p, P(u32), P(u32)]),
     "kc_graph_get_peel": (i32, [C.c_void_p, P(u32), P(u32)]),
     "kc_count": (i32, [C.c_void_p, P(KcParams), P(KcU128), P(KcCountStats)]),
+    "kc_count_shard": (i32, [C.c_void_p, P(KcParams), u32, u32, P(KcU128), P(KcCountStats)]),
     "kc_count_local": (i32, [C.c_void_p, P(KcParams), P(KcU128), P(KcU128)]),
     "kc_parse_spec": (i32, [C.c_char_p, P(KcParams)]),
     "kc_kcore": (i32, [C.c_void_p, P(u32), P(u32)]),

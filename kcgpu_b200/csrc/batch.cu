@@ -91,9 +91,18 @@ struct Choice {
   }
 };
 
-kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool device_input,
+// Where the edge arrays of run_batch live.
+enum class Input {
+  kHost,         // host memory: copied to device temporaries
+  kDevice,       // the caller's device memory: copied (the caller keeps it)
+  kDeviceOwned,  // device memory the call may overwrite (the batch pipeline's
+                 // staging buffers): used in place, edge_off[0] must be 0
+};
+
+kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, Input input,
                     const uint64_t* edge_off, const uint32_t* n_nodes, const uint32_t* ks, uint32_t G,
                     const kc_batch_opts* opts, kc_u128* counts, kc_params* choice, kc_batch_stats* stats) {
+  const bool device_input = input != Input::kHost;
   const double t0 = now_ms();
   cudaStream_t s = ctx->stream;
   if (G == 0) return KC_OK;
@@ -141,8 +150,14 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool 
   } release{&U, &plans, &cg, &cge, {e0, e1, e2, e3, e4, ec, eo}};
   uint32_t *ds = nullptr, *dd = nullptr, *dvoff = nullptr, *dnn = nullptr, *derr = nullptr, *vg = nullptr;
   unsigned long long* deoff = nullptr;
-  KC_CUDA(t.alloc(&ds, sizeof(uint32_t) * std::max<uint64_t>(1, E)));
-  KC_CUDA(t.alloc(&dd, sizeof(uint32_t) * std::max<uint64_t>(1, E)));
+  if (input == Input::kDeviceOwned) {
+    if (edge_off[0] != 0) return fail(KC_ERR_INTERNAL, "in-place batch input must start at edge 0");
+    ds = const_cast<uint32_t*>(src);
+    dd = const_cast<uint32_t*>(dst);
+  } else {
+    KC_CUDA(t.alloc(&ds, sizeof(uint32_t) * std::max<uint64_t>(1, E)));
+    KC_CUDA(t.alloc(&dd, sizeof(uint32_t) * std::max<uint64_t>(1, E)));
+  }
   KC_CUDA(t.alloc(&deoff, sizeof(unsigned long long) * ((size_t)G + 1)));
   KC_CUDA(t.alloc(&dvoff, sizeof(uint32_t) * ((size_t)G + 1)));
   KC_CUDA(t.alloc(&dnn, sizeof(uint32_t) * G));
@@ -151,7 +166,7 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool 
   std::vector<unsigned long long> eoff_rel((size_t)G + 1);
   for (uint32_t g = 0; g <= G; ++g) eoff_rel[g] = edge_off[g] - edge_off[0];
   cudaEventRecord(e0, s);
-  if (E) {
+  if (E && input != Input::kDeviceOwned) {
     const cudaMemcpyKind kind = device_input ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     KC_CUDA(cudaMemcpyAsync(ds, src + edge_off[0], sizeof(uint32_t) * E, kind, s));
     KC_CUDA(cudaMemcpyAsync(dd, dst + edge_off[0], sizeof(uint32_t) * E, kind, s));
@@ -216,10 +231,9 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool 
     for (uint32_t g = 0; g < G; ++g) {
       kc_params p;
       if (!opts || opts->autotune) {
-        p = autotune(n_nodes[g], fm[g], fmax[g], ks[g], fcore[g]);
+        p = autotune(n_nodes[g], fm[g], fmax[g], ks[g], fcore[g], orientation);
       } else {
-        p = opts->fixed;
-        if (p.part == 0) p.part = 8;
+        p = opts->fixed;  // part 0: each size class sizes its own partitions
       }
       p.k = ks[g];
       if (ks[g] <= 2) p.unit = KC_UNIT_NODE;  // an edge unit cannot count 1-cliques
@@ -371,6 +385,106 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, bool 
   return st;
 }
 
+// Host-input batches larger than the context's chunk size: chunks of whole
+// graphs of about that many edges are counted one after another, each as a
+// batch of its own (the graphs are independent), while the next chunk's edges
+// are copied to the device on the context's copy stream into the other of two
+// staging buffers. Each chunk is counted in place from its staging buffer.
+// Buffer b is refilled (for chunk c + 1) only after the chunk that used it
+// last (c - 1) has returned, and run_batch returns only once its stream is
+// idle.
+kc_status run_batch_pipelined(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, const uint64_t* edge_off,
+                              const uint32_t* n_nodes, const uint32_t* ks, uint32_t G, uint64_t chunk_edges,
+                              const kc_batch_opts* opts, kc_u128* counts, kc_params* choice,
+                              kc_batch_stats* stats) {
+  const double t0 = now_ms();
+  for (uint32_t g = 0; g < G; ++g)
+    if (edge_off[g + 1] < edge_off[g]) return fail(KC_ERR_INVALID_ARG, "edge_off decreases at graph %u", g);
+  std::vector<uint32_t> cut{0};  // chunk c holds graphs [cut[c], cut[c + 1])
+  for (uint32_t g = 0; g + 1 < G; ++g)
+    if (edge_off[g + 1] - edge_off[cut.back()] >= chunk_edges) cut.push_back(g + 1);
+  cut.push_back(G);
+  const uint32_t C = (uint32_t)cut.size() - 1;
+  uint64_t max_chunk = 1;
+  for (uint32_t c = 0; c < C; ++c) max_chunk = std::max<uint64_t>(max_chunk, edge_off[cut[c + 1]] - edge_off[cut[c]]);
+
+  cudaStream_t s = ctx->stream;
+  if (!ctx->copy) KC_CUDA(cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking));
+  DevTemps t(s);
+  uint32_t* buf[2][2] = {};
+  for (auto& b : buf)
+    for (auto& a : b) KC_CUDA(t.alloc(&a, sizeof(uint32_t) * max_chunk));
+  // events: the staging buffers allocated (stream-ordered on s), and the
+  // start / end of every chunk's copy; the guard (destroyed before t frees
+  // the buffers) waits for the copy stream on every return path
+  struct Guard {
+    cudaStream_t copy;
+    std::vector<cudaEvent_t> ev;
+    ~Guard() {
+      cudaStreamSynchronize(copy);
+      for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    }
+  } guard{ctx->copy, {}};
+  guard.ev.resize(1 + 2 * (size_t)C, nullptr);
+  for (auto& e : guard.ev) KC_CUDA(cudaEventCreate(&e));
+  cudaEvent_t ready = guard.ev[0];
+  auto cb = [&](uint32_t c) { return guard.ev[1 + 2 * (size_t)c]; };
+  auto ce = [&](uint32_t c) { return guard.ev[2 + 2 * (size_t)c]; };
+  KC_CUDA(cudaEventRecord(ready, s));
+  KC_CUDA(cudaStreamWaitEvent(ctx->copy, ready, 0));
+  auto issue_copy = [&](uint32_t c) -> kc_status {
+    const uint64_t e0 = edge_off[cut[c]], n = edge_off[cut[c + 1]] - e0;
+    KC_CUDA(cudaEventRecord(cb(c), ctx->copy));
+    if (n) {
+      KC_CUDA(cudaMemcpyAsync(buf[c & 1][0], src + e0, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, ctx->copy));
+      KC_CUDA(cudaMemcpyAsync(buf[c & 1][1], dst + e0, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, ctx->copy));
+    }
+    KC_CUDA(cudaEventRecord(ce(c), ctx->copy));
+    return KC_OK;
+  };
+  KC_TRY(issue_copy(0));
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  kc_batch_stats sum;
+  std::memset(&sum, 0, sizeof(sum));
+  std::vector<uint64_t> rel;
+  for (uint32_t c = 0; c < C; ++c) {
+    if (c + 1 < C) KC_TRY(issue_copy(c + 1));
+    KC_CUDA(cudaStreamWaitEvent(s, ce(c), 0));
+    const uint32_t g0 = cut[c], gn = cut[c + 1] - cut[c];
+    rel.resize((size_t)gn + 1);
+    for (uint32_t i = 0; i <= gn; ++i) rel[i] = edge_off[g0 + i] - edge_off[g0];
+    kc_batch_stats cs;
+    KC_TRY(run_batch(ctx, buf[c & 1][0], buf[c & 1][1], Input::kDeviceOwned, rel.data(), n_nodes + g0, ks + g0, gn,
+                     opts, counts + g0, choice ? choice + g0 : nullptr, stats ? &cs : nullptr));
+    if (!stats) continue;
+    sum.ms_build += cs.ms_build;
+    sum.ms_count += cs.ms_count;
+    sum.ms_csr += cs.ms_csr;
+    sum.ms_orient += cs.ms_orient;
+    sum.units += cs.units;
+    sum.kernels += cs.kernels;
+    sum.tree_nodes += cs.tree_nodes;
+    sum.word_ops += cs.word_ops;
+    sum.gather_bytes += cs.gather_bytes;
+    sum.heavy_units += cs.heavy_units;
+    for (int q = 0; q < 3; ++q) sum.cycles[q] += cs.cycles[q];
+    for (int q = 0; q < 5; ++q) sum.host_ms[q] += cs.host_ms[q];
+    sum.n_vertices += cs.n_vertices;
+    sum.n_edges += cs.n_edges;
+  }
+  KC_CUDA(cudaStreamSynchronize(ctx->copy));
+  if (stats) {
+    for (uint32_t c = 0; c < C; ++c) {
+      float ms = 0;
+      if (cudaEventElapsedTime(&ms, cb(c), ce(c)) == cudaSuccess) sum.ms_h2d += ms;
+    }
+    sum.n_graphs = G;
+    sum.ms_total = now_ms() - t0;
+    *stats = sum;
+  }
+  return KC_OK;
+}
+
 }  // namespace
 }  // namespace kc
 
@@ -384,7 +498,11 @@ kc_status kc_batch_count_packed(kc_ctx* ctx, const uint32_t* src, const uint32_t
   std::lock_guard<std::mutex> l(ctx->mu);
   cudaSetDevice(ctx->device);
   kc::clear_error();
-  return kc::run_batch(ctx, src, dst, false, edge_off, n_nodes, k, n_graphs, opts, counts, choice, stats);
+  const uint64_t chunk = ctx->batch_chunk_edges ? ctx->batch_chunk_edges : kc::kDefaultBatchChunkEdges;
+  if (src && dst && edge_off && n_nodes && k && counts && n_graphs > 1 && edge_off[n_graphs] >= edge_off[0] &&
+      edge_off[n_graphs] - edge_off[0] > chunk)
+    return kc::run_batch_pipelined(ctx, src, dst, edge_off, n_nodes, k, n_graphs, chunk, opts, counts, choice, stats);
+  return kc::run_batch(ctx, src, dst, kc::Input::kHost, edge_off, n_nodes, k, n_graphs, opts, counts, choice, stats);
 }
 
 kc_status kc_batch_count_packed_device(kc_ctx* ctx, const uint32_t* d_src, const uint32_t* d_dst,
@@ -395,7 +513,8 @@ kc_status kc_batch_count_packed_device(kc_ctx* ctx, const uint32_t* d_src, const
   std::lock_guard<std::mutex> l(ctx->mu);
   cudaSetDevice(ctx->device);
   kc::clear_error();
-  return kc::run_batch(ctx, d_src, d_dst, true, edge_off, n_nodes, k, n_graphs, opts, counts, choice, stats);
+  return kc::run_batch(ctx, d_src, d_dst, kc::Input::kDevice, edge_off, n_nodes, k, n_graphs, opts, counts, choice,
+                       stats);
 }
 
 kc_status kc_batch_count(kc_ctx* ctx, const kc_batch_graph* graphs, uint32_t n_graphs, const kc_batch_opts* opts,

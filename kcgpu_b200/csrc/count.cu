@@ -143,15 +143,21 @@ __global__ void __launch_bounds__(kPartThreads) k_class_scatter(const uint8_t* _
 }
 
 // [begin, count] of every class from the scanned chunk counts; also stamps the
-// pass's start on the global timer (the counting kernels' time limit).
+// pass's start on the global timer (the counting kernels' time limit). Unit
+// shard `shard` of S takes a class's positions shard, shard + S, ...: its
+// begin is the class start + shard, its count the positions left, and the
+// launches step through the queue by S (CountParams::qstride). Inside a class
+// units are in index order, so the stride deals out neighbouring units (and
+// the few largest ones) evenly between the shards.
 __global__ void k_class_bounds(const uint32_t* __restrict__ off, uint32_t n_chunks, uint32_t* bounds,
-                               unsigned long long* t0) {
+                               unsigned long long* t0, uint32_t shard, uint32_t n_shards) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   *t0 = global_ns();
   for (int c = 0; c < kNumClasses; ++c) {
     const uint32_t b = off[(size_t)c * n_chunks], e = off[(size_t)(c + 1) * n_chunks];
-    bounds[2 * c] = b;
-    bounds[2 * c + 1] = e - b;
+    const uint32_t cnt = e - b;
+    bounds[2 * c] = cnt > shard ? b + shard : b;
+    bounds[2 * c + 1] = cnt > shard ? (cnt - shard + n_shards - 1) / n_shards : 0u;
   }
 }
 
@@ -294,6 +300,7 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
     p.col = g->dcol;
     p.erow = g->erow;
     p.queue = heavy_pass ? pl->heavy : pl->queue;
+    p.qstride = heavy_pass ? 1u : std::max(1u, req.n_shards);
     p.bounds = pl->scratch + (heavy_pass ? kHeavyBounds : kClassBounds);
     p.cls = heavy_pass ? 0u : (uint32_t)c;
     p.n_units_max = pl->n_units;
@@ -349,7 +356,8 @@ kc_status count_enqueue(const CountPlan& pl, cudaStream_t s) {
   else KC_CUDA(cudaMemsetAsync(pl.ccnt, 0, sizeof(uint32_t) * kNumClasses * (size_t)nc, s));
   KC_CUDA(prim::scan_exclusive_u32(pl.ccnt, pl.ccnt, (size_t)kNumClasses * nc, s));
   k_class_bounds<<<1, 32, 0, s>>>(pl.ccnt, nc, pl.scratch + kClassBounds,
-                                  reinterpret_cast<unsigned long long*>(pl.scratch + kStartWord));
+                                  reinterpret_cast<unsigned long long*>(pl.scratch + kStartWord), pl.req.shard,
+                                  std::max(1u, pl.req.n_shards));
   if (pl.n_units) k_class_scatter<<<nc, kPartThreads, 0, s>>>(pl.cls, pl.n_units, nc, pl.ccnt, pl.queue);
   KC_CUDA(cudaGetLastError());
   // class launches side by side, then the heavy pass over the units they handed on

@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
 
   // class bounds come from device memory: clamp them so no unit index can leave the queue
   const uint32_t ubeg = min(p.bounds[2 * p.cls], p.n_units_max);
-  const uint32_t ucnt = min(p.bounds[2 * p.cls + 1], p.n_units_max - ubeg);
+  const uint32_t ucnt = min(p.bounds[2 * p.cls + 1], (p.n_units_max - ubeg + p.qstride - 1) / p.qstride);
   unsigned __int128 acc = 0;
   uint32_t acc_graph = 0xffffffffu;
   unsigned long long st_nodes = 0, st_words = 0, st_bytes = 0;
@@ -332,7 +332,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
     const uint32_t ui = hdr[0];
     if (ui >= ucnt) break;
     if (timing) tc = clk32();
-    const uint32_t unit = p.queue[ubeg + ui];
+    const uint32_t unit = p.queue[ubeg + (size_t)ui * p.qstride];
     uacc = 0;
     since_charge = 0;
     uint32_t src, d;

@@ -14,6 +14,7 @@ struct CountParams {
   const uint32_t* col;       // DAG columns, sorted per row
   const uint32_t* erow;      // source of every DAG edge (edge units)
   const uint32_t* queue;     // all units, largest first
+  uint32_t qstride;          // queue positions between this launch's units (the unit shards' count)
   const uint32_t* bounds;    // device [begin, count] per size class
   uint32_t cls;              // this launch's class
   uint32_t n_units_max;      // host upper bound on the class size (grid sizing)

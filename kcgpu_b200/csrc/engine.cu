@@ -15,6 +15,7 @@
 #include <string>
 #include <vector>
 
+#include "autotune_table.h"
 #include "count_kernels.cuh"
 #include "dev_common.cuh"
 #include "engine.h"
@@ -78,8 +79,47 @@ kc_status build_from_device(kc_graph* g, const uint32_t* d_src, const uint32_t* 
 
 }  // namespace
 
-kc_params autotune(uint32_t n, uint64_t m, uint32_t max_out, uint32_t k, uint32_t max_core) {
-  // Per-graph choice from shape features.
+namespace {
+
+uint32_t tune_band_u(uint32_t v, const uint32_t* lo, int n) {
+  int b = 0;
+  for (int i = 0; i < n; ++i)
+    if (v >= lo[i]) b = i;
+  return (uint32_t)b;
+}
+
+uint32_t tune_band_d(double v, const double* lo, int n) {
+  int b = 0;
+  for (int i = 0; i < n; ++i)
+    if (v >= lo[i]) b = i;
+  return (uint32_t)b;
+}
+
+}  // namespace
+
+kc_params autotune(uint32_t n, uint64_t m, uint32_t max_out, uint32_t k, uint32_t max_core, uint32_t orientation) {
+  // The measured table first: the fastest fixed method of the sweep for the
+  // graph's (k, largest out-degree, density) bucket, for degree-oriented
+  // graphs (the orientation the sweep measured).
+  const double dens0 = n > 1 ? (2.0 * (double)m) / ((double)n * (n - 1)) : 0.0;
+  if (orientation == KC_ORIENT_DEGREE && k >= 3) {
+    constexpr int nk = sizeof(tune::kKBands) / sizeof(tune::kKBands[0]);
+    constexpr int no = sizeof(tune::kOutBands) / sizeof(tune::kOutBands[0]);
+    constexpr int nd = sizeof(tune::kDensBands) / sizeof(tune::kDensBands[0]);
+    const tune::Entry& e = tune::kTable[tune_band_u(k, tune::kKBands, nk)][tune_band_u(max_out, tune::kOutBands, no)]
+                                       [tune_band_d(dens0, tune::kDensBands, nd)];
+    if (e.valid) {
+      kc_params p;
+      std::memset(&p, 0, sizeof(p));
+      p.k = k;
+      p.mode = e.mode;
+      p.unit = e.unit;
+      p.part = e.part;
+      p.encoding = e.encoding;
+      return p;
+    }
+  }
+  // Otherwise a choice from shape features.
   //  * mode: pivoting wins when the graph holds large cliques (its cost follows
   //    the clique tree, not the clique count); orientation listing wins on
   //    sparse neighbourhoods. A unit inside a c-core lists about C(c, k - 1)
@@ -194,6 +234,10 @@ kc_status kc_ctx_destroy(kc_ctx* ctx) {
       if (ctx->tend[c]) cudaEventDestroy(ctx->tend[c]);
     }
     if (ctx->fork) cudaEventDestroy(ctx->fork);
+    if (ctx->copy) {
+      cudaStreamSynchronize(ctx->copy);
+      cudaStreamDestroy(ctx->copy);
+    }
     ctx->cache.release(ctx->stream);
     cudaStreamSynchronize(ctx->stream);
     kc::unregister_stream_cache(ctx->stream);
@@ -207,6 +251,13 @@ kc_status kc_ctx_set_time_limit(kc_ctx* ctx, uint64_t ns) {
   if (!ctx) return fail(KC_ERR_INVALID_ARG, "context is NULL");
   std::lock_guard<std::mutex> l(ctx->mu);
   ctx->time_limit_ns = ns;
+  return KC_OK;
+}
+
+kc_status kc_ctx_set_batch_chunk_edges(kc_ctx* ctx, uint64_t edges) {
+  if (!ctx) return fail(KC_ERR_INVALID_ARG, "context is NULL");
+  std::lock_guard<std::mutex> l(ctx->mu);
+  ctx->batch_chunk_edges = edges;
   return KC_OK;
 }
 
@@ -381,11 +432,20 @@ kc_status kc_count(kc_graph* g, const kc_params* p, kc_u128* out, kc_count_stats
   return kc::count_on(g->ctx, g, p, out, stats);
 }
 
+kc_status kc_count_shard(kc_graph* g, const kc_params* p, uint32_t shard, uint32_t n_shards, kc_u128* out,
+                         kc_count_stats* stats) {
+  if (!g) return fail(KC_ERR_INVALID_ARG, "NULL argument");
+  if (n_shards == 0 || shard >= n_shards)
+    return fail(KC_ERR_INVALID_ARG, "shard %u of %u: need shard < n_shards", shard, n_shards);
+  return kc::count_on(g->ctx, g, p, out, stats, shard, n_shards);
+}
+
 }  // extern "C"
 
 namespace kc {
 
-kc_status count_on(kc_ctx* run, kc_graph* g, const kc_params* p, kc_u128* out, kc_count_stats* stats) {
+kc_status count_on(kc_ctx* run, kc_graph* g, const kc_params* p, kc_u128* out, kc_count_stats* stats,
+                   uint32_t shard, uint32_t n_shards) {
   if (!run || !g || !p || !out) return fail(KC_ERR_INVALID_ARG, "NULL argument");
   if (p->k < 1) return fail(KC_ERR_INVALID_ARG, "k must be >= 1");
   if (p->mode > KC_MODE_AUTO || p->unit > KC_UNIT_EDGE || p->encoding > KC_ENC_LIST)
@@ -398,8 +458,9 @@ kc_status count_on(kc_ctx* run, kc_graph* g, const kc_params* p, kc_u128* out, k
   kc::CtxLock lock(run);
   if (stats) std::memset(stats, 0, sizeof(*stats));
   out->lo = out->hi = 0;
-  if (p->k == 1) { out->lo = g->n; return KC_OK; }
-  if (p->k == 2) { out->lo = g->m; return KC_OK; }
+  // k <= 2 needs no units: the whole count belongs to shard 0
+  if (p->k == 1) { out->lo = shard == 0 ? g->n : 0; return KC_OK; }
+  if (p->k == 2) { out->lo = shard == 0 ? g->m : 0; return KC_OK; }
   cudaStream_t s = run->stream;
   kc::DevTemps t(s);
   unsigned long long* d_out = nullptr;
@@ -414,6 +475,8 @@ kc_status count_on(kc_ctx* run, kc_graph* g, const kc_params* p, kc_u128* out, k
   req.flags = p->flags;
   req.k_max = p->k;
   req.ctx = run;
+  req.shard = shard;
+  req.n_shards = n_shards;
   kc_status st = kc::count_graph(g, req, d_out, (p->flags & KC_FLAG_STATS) ? stats : nullptr);
   unsigned long long h[2] = {0, 0};
   if (st == KC_OK) {

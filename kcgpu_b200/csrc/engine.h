@@ -16,6 +16,11 @@ struct kc_ctx {
   int sms = 148;
   int max_smem_optin = 227 * 1024;
   uint64_t time_limit_ns = 0;  // device time limit of a counting pass (0 = none)
+  // host-input batches of more edges than this run as a pipeline of chunks of
+  // about this many edges, the next chunk's copy overlapping this one's work
+  // (0 = kc::kDefaultBatchChunkEdges, UINT64_MAX = never)
+  uint64_t batch_chunk_edges = 0;
+  cudaStream_t copy = nullptr;  // host->device copies of the batch pipeline (created on first use)
   kc::BlockCache cache;        // device blocks reused by allocations on `stream`
   uint64_t total_mem = 0;
   std::mutex mu;  // one call at a time per context
@@ -60,6 +65,9 @@ struct kc_graph {
 
 namespace kc {
 
+// 48M edges = 384 MB of u32 pairs, 6-7 ms of host->device copy on PCIe 5
+constexpr uint64_t kDefaultBatchChunkEdges = 48ull << 20;
+
 // A device allocation tracked against the graph's byte count.
 kc_status dev_alloc(kc_graph* g, void** p, size_t bytes);
 void dev_free(kc_graph* g, void* p);
@@ -85,6 +93,9 @@ struct CountRequest {
   // graph's own); another context of the same device may count a graph that
   // is complete (oriented, edge rows built), which the count then only reads
   kc_ctx* ctx = nullptr;
+  // unit shard: this count takes the units whose index inside their size
+  // class is = shard (mod n_shards); the shards' counts add up to the whole
+  uint32_t shard = 0, n_shards = 1;
 };
 
 // Runs the counting stage; d_out holds n_graphs (lo, hi) pairs and must be zeroed.
@@ -92,7 +103,8 @@ kc_status count_graph(kc_graph* g, const CountRequest& req, unsigned long long* 
                       kc_count_stats* stats);
 // kc_count run by the context `run` (its stream, scratch and lock) on a graph
 // of the same device; the graph must be complete (see CountRequest::ctx).
-kc_status count_on(kc_ctx* run, kc_graph* g, const kc_params* p, kc_u128* out, kc_count_stats* stats);
+kc_status count_on(kc_ctx* run, kc_graph* g, const kc_params* p, kc_u128* out, kc_count_stats* stats,
+                   uint32_t shard = 0, uint32_t n_shards = 1);
 // Completes an oriented graph for counting by other contexts: builds every
 // array a count could create lazily and waits for the graph's stream.
 kc_status complete_for_sharing(kc_graph* g);
@@ -103,6 +115,9 @@ kc_status truss_support(kc_graph* g, uint32_t* d_support);
 kc_status ensure_binom(kc_ctx* ctx, uint32_t rows, uint32_t cols);
 
 // Autotuner: the kc_params a graph of this shape runs best with.
-kc_params autotune(uint32_t n, uint64_t m, uint32_t max_out, uint32_t k, uint32_t max_core);
+// Per-graph method for the batched engine and the server: the measured table
+// (autotune_table.h) for degree-oriented graphs where its bucket was sampled,
+// the shape rule otherwise.
+kc_params autotune(uint32_t n, uint64_t m, uint32_t max_out, uint32_t k, uint32_t max_core, uint32_t orientation);
 
 }  // namespace kc

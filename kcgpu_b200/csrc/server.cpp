@@ -84,7 +84,7 @@ namespace {
 kc_params choose(const kc_server* s, const kc_graph_info& inf, uint32_t k) {
   kc_params p;
   if (s->opts.autotune) {
-    p = kc::autotune(inf.n, inf.m, inf.max_out_degree, k, inf.max_core);
+    p = kc::autotune(inf.n, inf.m, inf.max_out_degree, k, inf.max_core, s->opts.orientation);
   } else {
     p = s->opts.fixed;
     if (p.part == 0) p.part = 8;

@@ -5,7 +5,8 @@
   units past the limit; the call returns KC_ERR_DEVICE_TIMEOUT and the context
   counts correctly afterwards.
 * Allocation failure (kc_test_fail_alloc_after): every device allocation the
-  library makes is made to fail in turn; each failing call must return
+  library makes (single graphs, batches in one pass and as a pipeline of
+  chunks) is made to fail in turn; each failing call must return
   KC_ERR_OOM and leave no device allocation behind
   (kc_test_live_allocations), and the calls succeed again once the injection
   stops.
@@ -65,6 +66,11 @@ def _every_entry_point(ctx, s, d, n, bs, bd, off, nn, kk):
         g.orient("degree")
         out.append(g.count(4, mode="pivot", unit="edge", part=4))
     out.append(tuple(kc.batch_count(ctx, bs, bd, off, nn, kk)))
+    ctx.set_batch_chunk_edges(2000)  # the same batch as a pipeline of chunks
+    try:
+        out.append(tuple(kc.batch_count(ctx, bs, bd, off, nn, kk)))
+    finally:
+        ctx.set_batch_chunk_edges(0)
     return out
 
 

@@ -1,0 +1,69 @@
+"""Host side of counting one graph on several GPUs (kcgpu_b200.sharding): the
+128-bit limb arithmetic and the exact all-reduce of the shards' counts on
+world_size 2 with the gloo backend, on CPU."""
+import os
+import socket
+import sys
+from pathlib import Path
+
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = Path(__file__).resolve().parents[1]
+sys.path.insert(0, str(ROOT))
+
+from kcgpu_b200 import sharding  # noqa: E402
+
+
+@pytest.mark.parametrize("v", [0, 1, 2**32 - 1, 2**32, 2**64 - 1, 2**64, 2**127 + 12345, 2**128 - 1])
+def test_limbs_round_trip(v):
+    assert sharding.from_limb_sums(sharding.to_limbs(v)) == v
+
+
+def test_limb_sums_carry():
+    a, b = 2**128 - 2**40, 2**40 - 1
+    sums = [x + y for x, y in zip(sharding.to_limbs(a), sharding.to_limbs(b))]
+    assert sharding.from_limb_sums(sums) == 2**128 - 1
+    with pytest.raises(ValueError):
+        sharding.to_limbs(2**128)
+    with pytest.raises(OverflowError):
+        sharding.from_limb_sums([x + y for x, y in zip(sharding.to_limbs(2**128 - 1), sharding.to_limbs(1))])
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+CASES = [(2**128 - 1 - 987654321987654321, 987654321987654321), (2**64 - 1, 1), (0, 5), (2**96 + 7, 2**96 + 9)]
+
+
+def _rank(rank: int, world: int, port: int, out):
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    sys.path.insert(0, str(ROOT))
+    from kcgpu_b200 import sharding as sh
+
+    got = [sh.sum_u128(c[rank]) for c in CASES]
+    out.put((rank, got))
+    dist.destroy_process_group()
+
+
+def test_sum_u128_over_two_gloo_ranks():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    got = sorted(q.get(timeout=10) for _ in range(2))
+    want = [a + b for a, b in CASES]
+    assert got == [(0, want), (1, want)]
