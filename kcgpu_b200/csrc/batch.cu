@@ -30,20 +30,23 @@ namespace kc {
 
 namespace {
 
-__global__ void k_globalize(uint32_t* src, uint32_t* dst, const unsigned long long* __restrict__ eoff,
-                            const uint32_t* __restrict__ voff, const uint32_t* __restrict__ nn, uint32_t G,
-                            uint32_t* err) {
+// Local ids of graph g -> ids of the union (shifted by the vertices of the
+// graphs before g), from (in_s, in_d) into (out_s, out_d); in place when they
+// are the same arrays.
+__global__ void k_globalize(const uint32_t* in_s, const uint32_t* in_d, uint32_t* out_s, uint32_t* out_d,
+                            const unsigned long long* __restrict__ eoff, const uint32_t* __restrict__ voff,
+                            const uint32_t* __restrict__ nn, uint32_t G, uint32_t* err) {
   for (uint32_t g = blockIdx.x; g < G; g += gridDim.x) {
     const unsigned long long b = eoff[g], e = eoff[g + 1];
     const uint32_t off = voff[g], n = nn[g];
     for (unsigned long long i = b + threadIdx.x; i < e; i += blockDim.x) {
-      uint32_t u = src[i], v = dst[i];
+      uint32_t u = in_s[i], v = in_d[i];
       if (u >= n || v >= n) {
         atomicCAS(err, 0u, g + 1u);
         u = v = 0;
       }
-      src[i] = u + off;
-      dst[i] = v + off;
+      out_s[i] = u + off;
+      out_d[i] = v + off;
     }
   }
 }
@@ -94,7 +97,7 @@ struct Choice {
 // Where the edge arrays of run_batch live.
 enum class Input {
   kHost,         // host memory: copied to device temporaries
-  kDevice,       // the caller's device memory: copied (the caller keeps it)
+  kDevice,       // the caller's device memory: read in place, written global into temporaries
   kDeviceOwned,  // device memory the call may overwrite (the batch pipeline's
                  // staging buffers): used in place, edge_off[0] must be 0
 };
@@ -102,7 +105,6 @@ enum class Input {
 kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, Input input,
                     const uint64_t* edge_off, const uint32_t* n_nodes, const uint32_t* ks, uint32_t G,
                     const kc_batch_opts* opts, kc_u128* counts, kc_params* choice, kc_batch_stats* stats) {
-  const bool device_input = input != Input::kHost;
   const double t0 = now_ms();
   cudaStream_t s = ctx->stream;
   if (G == 0) return KC_OK;
@@ -166,16 +168,22 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, Input
   std::vector<unsigned long long> eoff_rel((size_t)G + 1);
   for (uint32_t g = 0; g <= G; ++g) eoff_rel[g] = edge_off[g] - edge_off[0];
   cudaEventRecord(e0, s);
-  if (E && input != Input::kDeviceOwned) {
-    const cudaMemcpyKind kind = device_input ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    KC_CUDA(cudaMemcpyAsync(ds, src + edge_off[0], sizeof(uint32_t) * E, kind, s));
-    KC_CUDA(cudaMemcpyAsync(dd, dst + edge_off[0], sizeof(uint32_t) * E, kind, s));
+  // host input is copied in and made global in place; device input is read
+  // where it lies and written global into the temporaries
+  const uint32_t* gin_s = ds;
+  const uint32_t* gin_d = dd;
+  if (E && input == Input::kHost) {
+    KC_CUDA(cudaMemcpyAsync(ds, src + edge_off[0], sizeof(uint32_t) * E, cudaMemcpyHostToDevice, s));
+    KC_CUDA(cudaMemcpyAsync(dd, dst + edge_off[0], sizeof(uint32_t) * E, cudaMemcpyHostToDevice, s));
+  } else if (input == Input::kDevice) {
+    gin_s = src + edge_off[0];
+    gin_d = dst + edge_off[0];
   }
   KC_CUDA(cudaMemcpyAsync(deoff, eoff_rel.data(), sizeof(unsigned long long) * ((size_t)G + 1), cudaMemcpyHostToDevice, s));
   KC_CUDA(cudaMemcpyAsync(dvoff, voff.data(), sizeof(uint32_t) * ((size_t)G + 1), cudaMemcpyHostToDevice, s));
   KC_CUDA(cudaMemcpyAsync(dnn, n_nodes, sizeof(uint32_t) * G, cudaMemcpyHostToDevice, s));
   cudaEventRecord(e1, s);
-  k_globalize<<<std::min<uint32_t>(G, 65535), 256, 0, s>>>(ds, dd, deoff, dvoff, dnn, G, derr);
+  k_globalize<<<std::min<uint32_t>(G, 65535), 256, 0, s>>>(gin_s, gin_d, ds, dd, deoff, dvoff, dnn, G, derr);
   uint32_t herr = 0;
   KC_CUDA(cudaMemcpyAsync(&herr, derr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   KC_CUDA(cudaStreamSynchronize(s));
@@ -278,6 +286,40 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, Input
       if (st != KC_OK) break;
     }
   }
+  // Passes of different methods are independent (each graph is in one pass):
+  // with more than one, pass i runs on its own stream with its own class
+  // streams, all forked from s and joined back to it, so the passes' long
+  // tails (a pass ends with its slowest unit) overlap instead of adding up.
+  if (st == KC_OK && plans.size() > 1) {
+    st = ensure_pass_streams(ctx, plans.size());
+    for (size_t i = 0; st == KC_OK && i < plans.size(); ++i)
+      for (int c = 0; c < kNumClasses; ++c) plans[i].side[c] = ctx->pool[i * (kNumClasses + 1) + 1 + c];
+  }
+  auto enqueue_passes = [&]() -> kc_status {
+    if (plans.size() == 1) return count_enqueue(plans[0], s);
+    KC_CUDA(cudaEventRecord(ctx->pool_fork, s));
+    kc_status r = KC_OK;
+    size_t forked = 0;
+    for (size_t i = 0; i < plans.size(); ++i) {
+      cudaStream_t ps = ctx->pool[i * (kNumClasses + 1)];
+      cudaError_t e = cudaStreamWaitEvent(ps, ctx->pool_fork, 0);
+      if (e != cudaSuccess) {
+        r = cuda_fail(e, "cudaStreamWaitEvent", __FILE__, __LINE__);
+        break;
+      }
+      ++forked;
+      r = count_enqueue(plans[i], ps);
+      if (r != KC_OK) break;
+    }
+    // every forked pass stream joins s, also after an error (a capture
+    // must end with every stream joined)
+    for (size_t i = 0; i < forked; ++i) {
+      cudaStream_t ps = ctx->pool[i * (kNumClasses + 1)];
+      cudaEventRecord(ctx->pool_done[i], ps);
+      cudaStreamWaitEvent(s, ctx->pool_done[i], 0);
+    }
+    return r;
+  };
   if (st == KC_OK) {
     KC_CUDA(cudaMemsetAsync(dout, 0, sizeof(unsigned long long) * 2 * G, s));
     KC_CUDA(cudaStreamSynchronize(s));
@@ -285,10 +327,7 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, Input
     const bool use_graph = !opts || opts->use_graph;
     if (use_graph) {
       KC_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-      for (auto& pl : plans) {
-        st = count_enqueue(pl, s);
-        if (st != KC_OK) break;
-      }
+      st = enqueue_passes();
       cudaError_t ce = cudaStreamEndCapture(s, &cg);
       if (st == KC_OK && ce != cudaSuccess) st = cuda_fail(ce, "cudaStreamEndCapture", __FILE__, __LINE__);
       if (st == KC_OK) {
@@ -303,10 +342,7 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, Input
       }
     } else {
       cudaEventRecord(e3, s);
-      for (auto& pl : plans) {
-        st = count_enqueue(pl, s);
-        if (st != KC_OK) break;
-      }
+      st = enqueue_passes();
       cudaEventRecord(e4, s);
     }
   }

@@ -207,11 +207,11 @@ void count_release(CountPlan* pl) {
   if (!pl->ctx) return;  // never prepared
   cudaStream_t s = pl->ctx->stream;
   for (int c = 0; c <= kNumClasses; ++c) release_launch(pl->launches[c], s);
-  void* ps[] = {pl->cls, pl->ccnt, pl->queue, pl->scratch, pl->heavy};
+  void* ps[] = {pl->cls, pl->ccnt, pl->queue, pl->scratch, pl->heavy, pl->help};
   for (void* p : ps)
     if (p) dfree(p, s);
   pl->cls = nullptr;
-  pl->ccnt = pl->queue = pl->scratch = pl->heavy = nullptr;
+  pl->ccnt = pl->queue = pl->scratch = pl->heavy = pl->help = nullptr;
 }
 
 // The context's side streams and events, created on first use.
@@ -227,6 +227,21 @@ static kc_status ensure_side(kc_ctx* ctx) {
     KC_CUDA(cudaEventCreate(&ctx->tend[c]));
   }
   KC_CUDA(cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming));
+  return KC_OK;
+}
+
+kc_status ensure_pass_streams(kc_ctx* ctx, size_t passes) {
+  if (!ctx->pool_fork) KC_CUDA(cudaEventCreateWithFlags(&ctx->pool_fork, cudaEventDisableTiming));
+  while (ctx->pool_done.size() < passes) {
+    for (int c = 0; c <= kNumClasses; ++c) {
+      cudaStream_t st = nullptr;
+      KC_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+      ctx->pool.push_back(st);
+    }
+    cudaEvent_t e = nullptr;
+    KC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ctx->pool_done.push_back(e);
+  }
   return KC_OK;
 }
 
@@ -262,6 +277,14 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
   KC_CUDA(dmalloc(&pl->queue, sizeof(uint32_t) * nu, s));
   KC_CUDA(dmalloc(&pl->heavy, sizeof(uint32_t) * nu, s));
   KC_CUDA(dmalloc(&pl->scratch, sizeof(uint32_t) * kScratchWords, s));
+  // Tail helping for the pivoting launches with a CTA per unit (classes 0
+  // and 1, the heavy pass): a cut-node ticket per queue position (the class
+  // queue, then the heavy list) and an active-unit word per CTA per launch.
+  const bool helping = req.mode != KC_MODE_ORIENT && req.encoding == KC_ENC_BITMAP && req.d_local == nullptr;
+  if (helping) {
+    pl->help_words = 2 * (size_t)nu + (size_t)(kNumClasses + 1) * kHelpMaxGrid;
+    KC_CUDA(dmalloc(&pl->help, sizeof(uint32_t) * pl->help_words, s));
+  }
   // Per-launch algorithm: orientation or pivot as requested; KC_MODE_AUTO
   // lists small units by orientation (cheap when their neighbourhood holds few
   // cliques) and counts large units and over-budget units with the pivot.
@@ -325,7 +348,15 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
       p.heavy_count = pl->scratch + kHeavyBounds + 1;
       any_budget = true;
     }
+    if (helping && lp.mode == KC_MODE_PIVOT && lp.G > 32u) {
+      p.help_ticket = pl->help + (heavy_pass ? nu : 0u);
+      p.help_active = pl->help + 2 * (size_t)nu + (size_t)c * kHelpMaxGrid;
+    }
     KC_TRY(prepare_launch(ctx, lp, p, s, &pl->launches[c]));
+    if (pl->launches[c].grid > kHelpMaxGrid) {  // (never on one B200: 148 SMs x 3 CTAs)
+      pl->launches[c].p.help_ticket = nullptr;
+      pl->launches[c].p.help_active = nullptr;
+    }
     pl->active[c] = true;
   }
   KC_TRY(ensure_side(ctx));
@@ -347,6 +378,7 @@ kc_status count_enqueue(const CountPlan& pl, cudaStream_t s) {
   kc_graph* g = pl.g;
   const int sms = pl.ctx->sms;
   KC_CUDA(cudaMemsetAsync(pl.scratch, 0, sizeof(uint32_t) * kScratchWords, s));
+  if (pl.help) KC_CUDA(cudaMemsetAsync(pl.help, 0, sizeof(uint32_t) * pl.help_words, s));
   const uint32_t gq = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((pl.n_units + 255) / 256, (uint64_t)sms * 16));
   if (pl.n_units)
     k_unit_class<<<gq, 256, 0, s>>>(g->drp, g->dcol, g->erow, pl.n_units, pl.edge ? 1 : 0, g->vgraph,

@@ -316,6 +316,14 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
   // pivoting keeps a (lo, hi) pair per vertex of S (counts of large cliques pass 2^64)
   auto loc2_add = [&](uint32_t i, unsigned __int128 v) { atomic_add_u128(loc + 2ull * i, v); };
 
+  // Tail helping: once the queue is empty, a CTA joins a unit that another
+  // CTA is still walking. Every walker of a unit (its owner's partitions and
+  // the helpers') walks the clique tree above the cut the same way and takes
+  // the nodes at the cut by a global ticket; only the owner's partition 0
+  // adds what lies above the cut. A walker that has been through all of the
+  // unit's cut nodes holds a ticket past the last one, so every cut node is
+  // taken: it sets bit 31 of the ticket, and no helper joins after that.
+  const bool help = MODE == 1 && !LOCAL && p.help_ticket != nullptr;
   for (;;) {
     if (gt == 0) {
       uint32_t tk = atomicAdd(p.ticket, 1u);
@@ -327,12 +335,37 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
       hdr[1] = 0;  // subtree ticket of this unit
       hdr[4] = 0;  // nodes charged to this unit
       hdr[5] = 0;  // unit over budget
+      hdr[6] = 0;  // helping: 1 + the queue position of the unit joined
     }
     gsync();
     const uint32_t ui = hdr[0];
-    if (ui >= ucnt) break;
+    size_t pos = ubeg + (size_t)ui * p.qstride;
+    bool helper = false;
+    if (ui >= ucnt) {
+      if (!help || ui == 0xffffffffu) break;
+      if (wig == 0) {  // the first warp looks for a unit still being walked
+        const uint32_t nb = gridDim.x;
+        uint32_t pick = 0;
+        for (uint32_t i0 = 0; i0 < nb && pick == 0u; i0 += 32u) {
+          uint32_t c = 0;
+          if (i0 + lane < nb) {
+            const uint32_t b = (blockIdx.x + 1u + i0 + lane) % nb;
+            const uint32_t a = *(volatile const uint32_t*)&p.help_active[b];
+            if (a != 0u && !(*(volatile const uint32_t*)&p.help_ticket[a - 1u] & 0x80000000u)) c = a;
+          }
+          const uint32_t m = __ballot_sync(0xffffffffu, c != 0u);
+          if (m) pick = __shfl_sync(0xffffffffu, c, __ffs(m) - 1);
+        }
+        if (lane == 0) hdr[6] = pick;
+      }
+      gsync();
+      const uint32_t a = hdr[6];
+      if (a == 0u) break;
+      helper = true;
+      pos = a - 1u;
+    }
     if (timing) tc = clk32();
-    const uint32_t unit = p.queue[ubeg + (size_t)ui * p.qstride];
+    const uint32_t unit = p.queue[pos];
     uacc = 0;
     since_charge = 0;
     uint32_t src, d;
@@ -412,7 +445,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
       // k - hold0 <= 1: the unit's count is 1 (the unit is the clique) or d
       const uint32_t hold0 = p.edge_units ? 2u : 1u;
       if (d == 0u || hold0 + d < k || k <= hold0 + 1u) {
-        if (part == 0 && k >= hold0 && hold0 + d >= k) acc += (k == hold0) ? 1u : d;
+        if (part == 0 && !helper && k >= hold0 && hold0 + d >= k) acc += (k == hold0) ? 1u : d;
         if (LOCAL && k >= hold0 && hold0 + d >= k && d <= p.dcap) {
           if (k == hold0 + 1u)
             for (uint32_t i = gt; i < d; i += G) atomic_add_u128(p.local + 2ull * S[i], 1u);
@@ -615,7 +648,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
     if (MODE == 1 && k == (p.edge_units ? 4u : 3u)) {
       // k - hold0 = 2: the unit's count is the number of edges of G[S]; a
       // vertex of S is in as many of those cliques as it has neighbours in S
-      if (part == 0) {
+      if (part == 0 && !helper) {
         unsigned long long e2 = 0;  // twice the edges: the bitmap is symmetric
         for (uint32_t j = pt.plane; j < d; j += pt.P) {
           uint32_t dj = 0;
@@ -946,15 +979,22 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
       // partition 0 alone adds what the nodes above the cut contribute.
       // L grows when the root has few branches (dense units, whose pivot
       // neighbours nearly everything).
-      const uint32_t nparts = G / pt.P;
+      // With tail helping the cut is sized for helpers too (four CTAs' worth
+      // of partitions), the same for every walker of the unit.
+      const uint32_t nparts = (G / pt.P) * (help ? 4u : 1u);
       uint32_t nr0 = 0;
       for (uint32_t w = pt.plane; w < W; w += pt.P) nr0 += __popc(R0[w]);
       nr0 = __reduce_add_sync(pt.pmask, nr0);
       const uint32_t L = (nparts == 1u || nr0 >= 4u * nparts) ? 1u : (nr0 <= 2u ? 3u : 2u);
-      const bool top_owner = part == 0u;
+      const bool top_owner = part == 0u && !helper;
+      uint32_t* cut_ticket = help ? p.help_ticket + pos : &hdr[1];
+      if (help && !helper && gt == 0) {  // the unit can take helpers from now on
+        __threadfence();
+        *(volatile uint32_t*)&p.help_active[blockIdx.x] = (uint32_t)pos + 1u;
+      }
       auto ticket = [&]() -> uint32_t {
         uint32_t t = 0;
-        if (pt.plane == 0) t = atomicAdd(&hdr[1], 1u);
+        if (pt.plane == 0) t = atomicAdd(cut_ticket, 1u);
         return __shfl_sync(pt.pmask, t, pt.pbase);
       };
       uint32_t seen = 0, mine = ticket();
@@ -1110,9 +1150,12 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
           }
         }
       }
+      // this walker has been through every cut node: all of them are taken
+      if (help && pt.plane == 0) atomicOr(cut_ticket, 0x80000000u);
     }
     gsync();
     lap(2);
+    if (help && !helper && gt == 0) *(volatile uint32_t*)&p.help_active[blockIdx.x] = 0u;
     // commit the unit, or hand it to the heavy pass when it ran over budget
     if (budgeted && hdr[5]) {
       if (gt == 0) p.heavy[atomicAdd(p.heavy_count, 1u)] = unit;

@@ -53,6 +53,12 @@ struct CountParams {
   uint32_t budget;           // traversal nodes a unit may use before it is handed on (0 = no limit)
   uint32_t* heavy;           // units over budget, counted again by the heavy pass
   uint32_t* heavy_count;     // their number (atomic)
+  // Tail helping (pivoting, a CTA per unit, no local counts; null = off):
+  // the cut-node ticket of every queue position (bit 31 once every cut node
+  // of the unit is claimed), and per CTA of the launch 1 + the queue
+  // position of the unit it walks (0 = none).
+  uint32_t* help_ticket;
+  uint32_t* help_active;
 };
 
 struct LaunchPlan {
@@ -92,7 +98,8 @@ void release_launch(PreparedLaunch& pl, cudaStream_t s);
 constexpr int kNumClasses = 4;
 constexpr uint32_t kWarpClassMax = 128;   // largest unit a warp group takes
 constexpr uint32_t kUnitBudget = 8192;    // traversal nodes before a warp unit is handed on
-constexpr size_t kStaticSmemBytes = 64;   // static shared memory of the bitmap kernel (phase clocks), kept off the plan
+constexpr size_t kStaticSmemBytes = 64;
+constexpr uint32_t kHelpMaxGrid = 2048;   // most CTAs of a launch that takes part in tail helping   // static shared memory of the bitmap kernel (phase clocks), kept off the plan
 
 // Layout of a plan's scratch words (zeroed by every enqueue).
 constexpr uint32_t kScratchWords = 48;
@@ -117,6 +124,8 @@ struct CountPlan {
   uint32_t n_chunks = 0;
   uint32_t *queue = nullptr, *scratch = nullptr;
   uint32_t* heavy = nullptr;
+  uint32_t* help = nullptr;  // tail-helping words (zeroed by every enqueue), help_words of them
+  size_t help_words = 0;
   unsigned long long* d_out = nullptr;
   PreparedLaunch launches[kNumClasses + 1];
   bool active[kNumClasses + 1] = {false, false, false, false, false};

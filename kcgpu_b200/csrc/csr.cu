@@ -46,8 +46,10 @@ __device__ __forceinline__ uint32_t grouped_add(uint32_t* ctr, uint32_t key, uin
   return base + (uint32_t)__popc(peers & lanemask_lt());
 }
 
+// Also checks every endpoint against n (a known vertex count): an edge with
+// an endpoint >= n sets *bad to 1 and is not counted (the build then fails).
 __global__ void k_degree(const uint32_t* __restrict__ src, const uint32_t* __restrict__ dst, uint64_t E,
-                         uint32_t* deg) {
+                         uint32_t n, uint32_t* deg, uint32_t* bad) {
   const uint32_t lane = lane_id();
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); b < E; b += stride) {
@@ -56,6 +58,10 @@ __global__ void k_degree(const uint32_t* __restrict__ src, const uint32_t* __res
     if (i < E) {
       u = src[i];
       v = dst[i];
+      if (u >= n || v >= n) {
+        atomicOr(bad, 1u);
+        u = v = 0xffffffffu;
+      }
       if (u == v) u = v = 0xffffffffu;
     }
     grouped_add(deg, u, lane);
@@ -104,18 +110,15 @@ kc_status build_csr(kc_graph* g, const uint32_t* d_src, const uint32_t* d_dst, u
   KC_CUDA(tmp.alloc(&scal, 4 * sizeof(uint32_t)));
   KC_CUDA(cudaMemsetAsync(scal, 0, 4 * sizeof(uint32_t), s));
   uint32_t h[4] = {0, 0, 0, 0};
-  if (E) {
+  // scal[3]: an endpoint >= n was seen (checked by k_degree)
+  uint32_t n = n_nodes;
+  if (n == 0 && E) {  // n from the largest id; a known n needs no extra pass
     k_max_id<<<grid_e, 256, 0, s>>>(d_src, d_dst, E, scal);
     KC_CUDA(cudaGetLastError());
     KC_CUDA(cudaMemcpyAsync(h, scal, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     KC_CUDA(cudaStreamSynchronize(s));
-  }
-  uint32_t n = n_nodes;
-  if (n == 0) {
-    if (E && h[0] == 0xffffffffu) return fail(KC_ERR_INVALID_ARG, "vertex id 0xffffffff is reserved");
-    n = E ? h[0] + 1 : 0;
-  } else if (E && h[0] >= n) {
-    return fail(KC_ERR_INVALID_ARG, "edge endpoint %u is not below n_nodes = %u", h[0], n);
+    if (h[0] == 0xffffffffu) return fail(KC_ERR_INVALID_ARG, "vertex id 0xffffffff is reserved");
+    n = h[0] + 1;
   }
   if (2 * E >= 0xffffffffull)
     return fail(KC_ERR_INVALID_ARG, "%llu input edges exceed the 32-bit offset range", (unsigned long long)E);
@@ -125,13 +128,14 @@ kc_status build_csr(kc_graph* g, const uint32_t* d_src, const uint32_t* d_dst, u
   KC_CUDA(tmp.alloc(&deg, sizeof(uint32_t) * ((size_t)n + 1)));
   KC_CUDA(tmp.alloc(&off, sizeof(uint32_t) * ((size_t)n + 1)));
   KC_CUDA(cudaMemsetAsync(deg, 0, sizeof(uint32_t) * ((size_t)n + 1), s));
-  if (E) k_degree<<<grid_e, 256, 0, s>>>(d_src, d_dst, E, deg);
+  if (E) k_degree<<<grid_e, 256, 0, s>>>(d_src, d_dst, E, n, deg, scal + 3);
   KC_CUDA(prim::scan_exclusive_u32(deg, off, n, s));
   uint32_t total = 0;
   KC_CUDA(cudaMemcpyAsync(&total, off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   if (n) k_max_row<<<std::max(1u, std::min((n + 255) / 256, (uint32_t)sms * 8)), 256, 0, s>>>(off, n, scal + 1);
-  KC_CUDA(cudaMemcpyAsync(h + 1, scal + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  KC_CUDA(cudaMemcpyAsync(h + 1, scal + 1, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   KC_CUDA(cudaStreamSynchronize(s));
+  if (h[3]) return fail(KC_ERR_INVALID_ARG, "an edge endpoint is not below n_nodes = %u", n);
 
   KC_CUDA(tmp.alloc(&adj, sizeof(uint32_t) * std::max<size_t>(1, total)));
   // deg is reused as the scatter cursor (a copy of the offsets)

@@ -238,6 +238,12 @@ kc_status kc_ctx_destroy(kc_ctx* ctx) {
       cudaStreamSynchronize(ctx->copy);
       cudaStreamDestroy(ctx->copy);
     }
+    for (cudaStream_t st : ctx->pool) {
+      cudaStreamSynchronize(st);
+      cudaStreamDestroy(st);
+    }
+    for (cudaEvent_t e : ctx->pool_done) cudaEventDestroy(e);
+    if (ctx->pool_fork) cudaEventDestroy(ctx->pool_fork);
     ctx->cache.release(ctx->stream);
     cudaStreamSynchronize(ctx->stream);
     kc::unregister_stream_cache(ctx->stream);

@@ -33,6 +33,12 @@ struct kc_ctx {
   cudaStream_t side[kSide] = {};
   cudaEvent_t fork = nullptr, join[kSide] = {};
   cudaEvent_t tbeg[kSide + 1] = {}, tend[kSide + 1] = {};  // per-launch timing
+  // a batch's counting passes (one per method) run side by side: pass i on
+  // pool[i (1 + kSide)], its class launches on the next kSide streams; done[i]
+  // joins pass i back to `stream` (created on first use, grown as needed)
+  std::vector<cudaStream_t> pool;
+  std::vector<cudaEvent_t> pool_done;
+  cudaEvent_t pool_fork = nullptr;
 };
 
 struct kc_graph {
@@ -78,6 +84,8 @@ kc_status build_csr(kc_graph* g, const uint32_t* d_src, const uint32_t* d_dst, u
                     uint32_t n_nodes);
 kc_status orient_graph(kc_graph* g, uint32_t orientation);
 kc_status ensure_edge_rows(kc_graph* g);
+// Grows the context's pass streams to hold `passes` counting passes side by side.
+kc_status ensure_pass_streams(kc_ctx* ctx, size_t passes);
 kc_status peel_graph(kc_graph* g);  // fills prio / level / max_core
 
 struct CountRequest {

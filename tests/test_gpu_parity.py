@@ -262,3 +262,24 @@ def test_units_above_1024_vertices(ctx):
             want = G.multipartite_kcliques(sizes, k)
             for mode, unit, enc in VARIANTS:
                 assert g.count(k, mode=mode, unit=unit, encoding=enc) == want, (k, mode, unit, enc)
+
+
+def test_pivot_cta_units_with_tail_helping(ctx):
+    """Four dense blocks (p 0.5, 350 vertices each): a few dozen units above
+    128 vertices, counted by a CTA each with pivoting, far fewer than the
+    launch's CTAs, so most CTAs join units still being walked (tail helping)
+    and take cut nodes by the unit's global ticket. Every count equals the
+    oracle's, in every pivoting variant and partition size."""
+    s, d, n = kc.gen_sbm(1400, 4, 0.5, 0.001, 7).arrays()
+    og = OracleGraph(s, d, n)
+    assert og.orient("degen") > 128
+    with kc.Graph.from_edges(ctx, s, d, n) as g:
+        g.orient("degen")
+        for k in (6, 9):
+            want = og.count(k, "pivot", closed=True)
+            for mode in ("pivot", "auto"):
+                for unit in ("node", "edge"):
+                    for part in (4, 32):
+                        assert g.count(k, mode=mode, unit=unit, part=part) == want, (k, mode, unit, part)
+            # repeated counts agree (helpers join at different moments each time)
+            assert [g.count(k, mode="pivot", unit="node", part=32) for _ in range(3)] == [want] * 3
