@@ -41,7 +41,7 @@ def _fixture(name):
     return fx[name]
 
 
-def _check_single(ctx, name, mode, unit, part):
+def _check_single(ctx, name, mode, unit, part, max_k=99):
     rec = _fixture(name)
     _, s, d, n, orient, _, _ = MCG.graph_spec(name)
     assert MCG.sha_arrays(s, d) == rec["input_sha256"], f"{name}: generator output changed"
@@ -49,6 +49,8 @@ def _check_single(ctx, name, mode, unit, part):
         g.orient(orient)
         assert g.info()["m"] == rec["m"]
         for k, want in rec["counts"].items():
+            if int(k) > max_k:
+                continue
             got = g.count(int(k), mode=mode, unit=unit, part=part, encoding="bitmap")
             assert got == int(want), (name, k, got, want)
     return rec
@@ -68,7 +70,9 @@ def test_rmat_scale20_edge_factor16(ctx):
 
 
 def test_chung_lu_4m_planted_cliques(ctx):
-    rec = _check_single(ctx, "chunglu4m", "pivot", "node", 0)
+    # k <= 9 here (about 40 s of device time); the fixture's k = 10 is checked
+    # by bench.py --workload chunglu --ks 10 (oracle_fixture in its line)
+    rec = _check_single(ctx, "chunglu4m", "pivot", "node", 0, max_k=9)
     for k, want in rec["counts"].items():
         assert int(want) >= 200 * math.comb(30, int(k))  # 200 disjoint planted cliques of >= 30 vertices
 
