@@ -75,6 +75,8 @@ def parse():
     ap.add_argument("--streams", type=int, default=8, help="serving: worker contexts / streams")
     ap.add_argument("--no-serving", action="store_true", help="batched workload: skip the serving leg")
     ap.add_argument("--tune-sample", type=int, default=1500, help="batched: graphs of the autotuner comparison")
+    ap.add_argument("--batch-chunk-edges", type=int, default=0,
+                    help="batched e2e: pipeline chunk size in edges (0 = the library default, -1 = one pass)")
     ap.add_argument("--tune-time-limit", type=float, default=5.0,
                     help="batched: device seconds per counting pass in the autotuner comparison")
     return ap.parse_args()
@@ -513,6 +515,7 @@ def main():
     import kcgpu_b200 as kc
 
     ctx = kc.Context(local)
+    ctx.set_batch_chunk_edges(2**64 - 1 if args.batch_chunk_edges < 0 else args.batch_chunk_edges)
     L = kc.lib()
     el, s, d, off, nn, kk, fam = make_batch(kc, args.graphs, args.seed + rank * args.graphs)
     G = len(nn)

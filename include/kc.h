@@ -145,7 +145,7 @@ kc_status kc_ctx_set_time_limit(kc_ctx* ctx, uint64_t ns);
  * chunk's edges are copied to the device on a second stream, so the
  * host->device copy of all but the first chunk is hidden behind device work.
  * Counts and choices are the same as in one pass; kc_batch_stats add up the
- * chunks (ms_h2d is the copy stream's time). 0 = the default (48M edges),
+ * chunks (ms_h2d is the copy stream's time). 0 = the default (96M edges),
  * UINT64_MAX = never split. Device-input batches always run in one pass. */
 kc_status kc_ctx_set_batch_chunk_edges(kc_ctx* ctx, uint64_t edges);
 /* Device memory the context keeps for reuse: the engine's temporaries and the

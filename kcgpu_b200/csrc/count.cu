@@ -174,8 +174,12 @@ uint32_t auto_part(uint32_t mode, uint32_t W) {
 
 kc_status ensure_binom(kc_ctx* ctx, uint32_t rows, uint32_t cols) {
   if (ctx->d_binom && ctx->brows >= rows && ctx->bcols >= cols) return KC_OK;
-  rows = std::max(rows, ctx->brows);
-  cols = std::max(cols, ctx->bcols);
+  // Grown in large steps (rows to a power of two, at least 128; at least 34
+  // columns, k up to 33), so a context regrows it a few times at most.
+  uint32_t r2 = 128;
+  while (r2 < std::max(rows, ctx->brows)) r2 <<= 1;
+  rows = r2;
+  cols = std::max<uint32_t>(std::max(cols, ctx->bcols), 34u);
   std::vector<unsigned __int128> t((size_t)(rows + 1) * (cols + 1), 0);
   for (uint32_t r = 0; r <= rows; ++r) {
     t[(size_t)r * (cols + 1)] = 1;
@@ -187,16 +191,21 @@ kc_status ensure_binom(kc_ctx* ctx, uint32_t rows, uint32_t cols) {
     h[2 * i] = (unsigned long long)t[i];
     h[2 * i + 1] = (unsigned long long)(t[i] >> 64);
   }
-  // the new table replaces the old one only once it is complete
+  // The new table replaces the old one once it is complete. Everything is
+  // ordered on the context's own stream: no call here waits for the whole
+  // device (a cudaFree would, stalling every other context's work). The old
+  // table stays allocated until the context is destroyed: a plan prepared
+  // before the growth may still point at it.
   unsigned long long* nb = nullptr;
-  KC_CUDA(cudaMalloc(&nb, h.size() * sizeof(unsigned long long)));
-  const cudaError_t e = cudaMemcpy(nb, h.data(), h.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice);
+  KC_CUDA(dmalloc(&nb, h.size() * sizeof(unsigned long long), ctx->stream));
+  cudaError_t e = cudaMemcpyAsync(nb, h.data(), h.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                                  ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);  // (h is freed on return)
   if (e != cudaSuccess) {
-    cudaFree(nb);
+    dfree(nb, ctx->stream);
     return cuda_fail(e, "binomial table upload", __FILE__, __LINE__);
   }
-  cudaStreamSynchronize(ctx->stream);
-  if (ctx->d_binom) cudaFree(ctx->d_binom);
+  if (ctx->d_binom) ctx->binom_retired.push_back(ctx->d_binom);
   ctx->d_binom = nb;
   ctx->brows = rows;
   ctx->bcols = cols;

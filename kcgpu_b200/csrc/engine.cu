@@ -223,7 +223,8 @@ kc_status kc_ctx_destroy(kc_ctx* ctx) {
     std::lock_guard<std::mutex> l(ctx->mu);
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    if (ctx->d_binom) cudaFree(ctx->d_binom);
+    if (ctx->d_binom) kc::dfree(ctx->d_binom, ctx->stream);
+    for (unsigned long long* b : ctx->binom_retired) kc::dfree(b, ctx->stream);
     for (int c = 0; c < kc_ctx::kSide; ++c) {
       if (ctx->side[c]) cudaStreamSynchronize(ctx->side[c]);
       if (ctx->side[c]) cudaStreamDestroy(ctx->side[c]);

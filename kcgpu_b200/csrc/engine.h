@@ -27,6 +27,7 @@ struct kc_ctx {
   // exact binomial table C(r, c) as (lo, hi) pairs, rows [0, brows], cols [0, bcols]
   unsigned long long* d_binom = nullptr;
   uint32_t brows = 0, bcols = 0;
+  std::vector<unsigned long long*> binom_retired;  // earlier, smaller tables (freed with the context)
   // the counting pass's size classes run side by side on these streams
   // (created on first use; calls on one context are serialised by mu)
   static constexpr int kSide = 4;
@@ -71,8 +72,9 @@ struct kc_graph {
 
 namespace kc {
 
-// 48M edges = 384 MB of u32 pairs, 6-7 ms of host->device copy on PCIe 5
-constexpr uint64_t kDefaultBatchChunkEdges = 48ull << 20;
+// 96M edges = 768 MB of u32 pairs, about 13 ms of host->device copy at 57 GB/s:
+// few chunks, so their fixed costs (a counting tail each) stay small
+constexpr uint64_t kDefaultBatchChunkEdges = 96ull << 20;
 
 // A device allocation tracked against the graph's byte count.
 kc_status dev_alloc(kc_graph* g, void** p, size_t bytes);
