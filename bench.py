@@ -525,13 +525,16 @@ def main():
     torch.cuda.synchronize()
     stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=f"cuda:{local}")
 
-    def run_device():
-        return kc.batch_count(ctx, None, None, off, nn, kk, orientation="degree", autotune=True, use_graph=True,
-                              return_choice=True, return_stats=True, device_ptrs=(d_s.data_ptr(), d_d.data_ptr()))
+    def run_device(with_choice=False):
+        # the per-graph choices (10,000 dicts) are read once, after the timed steps
+        r = kc.batch_count(ctx, None, None, off, nn, kk, orientation="degree", autotune=True, use_graph=True,
+                           return_choice=with_choice, return_stats=True,
+                           device_ptrs=(d_s.data_ptr(), d_d.data_ptr()))
+        return r if with_choice else (r[0], None, r[1])
 
     def run_host():
         return kc.batch_count(ctx, s, d, off, nn, kk, orientation="degree", autotune=True, use_graph=True,
-                              return_choice=True, return_stats=True)
+                              return_stats=True)
 
     for _ in range(args.warmup):
         counts, choice, st = run_device()
@@ -573,13 +576,14 @@ def main():
         ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
         for i in range(args.steps):
             ev2[i][0].record(stream)
-            counts_h, _, _ = run_host()
+            counts_h, _ = run_host()
             ev2[i][1].record(stream)
         torch.cuda.synchronize()
         e2e_ms = max_over_ranks(pg, sum(a.elapsed_time(b) for a, b in ev2) / args.steps, local)
         e2e_val = world * G / (e2e_ms / 1e3)
         assert counts_h == counts, "host-input and device-input batches disagree"
 
+    _, choice, _ = run_device(with_choice=True)  # the autotuner's choices, untimed
     total_cliques = sum(counts)
     out = None
     if rank == 0:

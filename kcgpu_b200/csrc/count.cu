@@ -288,10 +288,12 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
   KC_CUDA(dmalloc(&pl->scratch, sizeof(uint32_t) * kScratchWords, s));
   // Tail helping for the pivoting launches with a CTA per unit (classes 0
   // and 1, the heavy pass): a cut-node ticket per queue position (the class
-  // queue, then the heavy list) and an active-unit word per CTA per launch.
+  // queue, then the heavy list), an active-unit word per CTA per launch, and
+  // the exited CTAs of each class launch.
   const bool helping = req.mode != KC_MODE_ORIENT && req.encoding == KC_ENC_BITMAP && req.d_local == nullptr;
+  const size_t exit_at = 2 * (size_t)nu + (size_t)(kNumClasses + 1) * kHelpMaxGrid;
   if (helping) {
-    pl->help_words = 2 * (size_t)nu + (size_t)(kNumClasses + 1) * kHelpMaxGrid;
+    pl->help_words = exit_at + kNumClasses;
     KC_CUDA(dmalloc(&pl->help, sizeof(uint32_t) * pl->help_words, s));
   }
   // Per-launch algorithm: orientation or pivot as requested; KC_MODE_AUTO
@@ -361,6 +363,7 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
       p.help_ticket = pl->help + (heavy_pass ? nu : 0u);
       p.help_active = pl->help + 2 * (size_t)nu + (size_t)c * kHelpMaxGrid;
     }
+    if (helping && !heavy_pass) p.class_exit = pl->help + exit_at;  // grids filled in below
     KC_TRY(prepare_launch(ctx, lp, p, s, &pl->launches[c]));
     if (pl->launches[c].grid > kHelpMaxGrid) {  // (never on one B200: 148 SMs x 3 CTAs)
       pl->launches[c].p.help_ticket = nullptr;
@@ -368,6 +371,11 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
     }
     pl->active[c] = true;
   }
+  if (helping)
+    for (int c = 0; c < kNumClasses; ++c)
+      if (pl->active[c])
+        for (int o = 0; o < kNumClasses; ++o)
+          pl->launches[c].p.class_grid[o] = pl->active[o] ? pl->launches[o].grid : 0u;
   KC_TRY(ensure_side(ctx));
   for (int c = 0; c < kNumClasses; ++c) {
     pl->side[c] = ctx->side[c];

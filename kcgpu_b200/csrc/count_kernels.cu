@@ -343,6 +343,21 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
     bool helper = false;
     if (ui >= ucnt) {
       if (!help || ui == 0xffffffffu) break;
+      // A CTA of a class launch helps only once the plan's other class
+      // launches have finished (all their CTAs exited): while they run, its
+      // slot serves them better than a share of another CTA's unit. The
+      // heavy pass runs alone and always helps.
+      if (p.class_exit != nullptr) {
+        uint32_t busy = 0;
+        if (gt == 0)
+          for (int c = 0; c < kNumClasses; ++c)
+            if (c != (int)p.cls && p.class_grid[c] != 0u &&
+                *(volatile const uint32_t*)&p.class_exit[c] < p.class_grid[c])
+              busy = 1;
+        if (gt == 0) hdr[7] = busy;
+        gsync();
+        if (hdr[7]) break;
+      }
       if (wig == 0) {  // the first warp looks for a unit still being walked
         const uint32_t nb = gridDim.x;
         uint32_t pick = 0;
@@ -979,9 +994,11 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
       // partition 0 alone adds what the nodes above the cut contribute.
       // L grows when the root has few branches (dense units, whose pivot
       // neighbours nearly everything).
-      // With tail helping the cut is sized for helpers too (four CTAs' worth
-      // of partitions), the same for every walker of the unit.
-      const uint32_t nparts = (G / pt.P) * (help ? 4u : 1u);
+      // The cut is sized for the CTA's own partitions (helpers take what is
+      // left of it): a deeper cut would make every walker, helpers included,
+      // walk more levels above it, and on bushy trees that costs more than
+      // the finer split gains.
+      const uint32_t nparts = G / pt.P;
       uint32_t nr0 = 0;
       for (uint32_t w = pt.plane; w < W; w += pt.P) nr0 += __popc(R0[w]);
       nr0 = __reduce_add_sync(pt.pmask, nr0);
@@ -1186,6 +1203,13 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
     gsync();
   }
   flush();
+  if (p.class_exit != nullptr) {  // this CTA is done: count it out of its class launch
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicAdd(&p.class_exit[p.cls], 1u);
+    }
+  }
   if (p.stats && pt.plane == 0) {
     atomicAdd(p.stats + 0, st_nodes);
     atomicAdd(p.stats + 1, st_words);

@@ -59,6 +59,10 @@ struct CountParams {
   // position of the unit it walks (0 = none).
   uint32_t* help_ticket;
   uint32_t* help_active;
+  // Class launches that help: CTAs that have exited, per class launch of the
+  // plan, and each launch's grid (0 = not launched); null for the heavy pass
+  uint32_t* class_exit;
+  uint32_t class_grid[4];
 };
 
 struct LaunchPlan {
