@@ -199,6 +199,14 @@ kc_status kc_graph_get_peel(const kc_graph* g, uint32_t* priority, uint32_t* lev
 
 /* ---- counting -------------------------------------------------------- */
 kc_status kc_count(kc_graph* g, const kc_params* p, kc_u128* out, kc_count_stats* stats);
+/* The counts for several k of one graph in one walk: out[i] = the number of
+ * ks[i]-cliques, for n_k <= 32 values of k in any order (repeats allowed).
+ * Pivoting with the binary encoding and p->unit (p->mode and p->part are
+ * not used): the succinct clique tree is walked once to the largest k, and
+ * every smaller k is taken where it closes (k - held <= 2) or at the leaves,
+ * so the call costs about as much as kc_count at the largest k. No reference
+ * counterpart (the reference counts one k per run, src/main.cu:263-588). */
+kc_status kc_count_multi(kc_graph* g, const kc_params* p, const uint32_t* ks, uint32_t n_k, kc_u128* out);
 /* One unit shard of kc_count, for counting one graph on several GPUs (each
  * process holds the whole graph and counts its shard; the caller adds the
  * shards' counts, e.g. with an all-gather of the 16-byte results). Units are

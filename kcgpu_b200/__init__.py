@@ -219,6 +219,19 @@ class Graph:
             return CountResult(out.value(), vals)
         return out.value()
 
+    def count_multi(self, ks, unit="node") -> list:
+        """Exact counts for several k in one pivoting walk (kc_count_multi):
+        a list in the order of ks."""
+        kk = _as_u32(list(ks))
+        p = KcParams()
+        p.k = int(kk.max()) if kk.size else 0
+        p.mode = MODES["pivot"]
+        p.unit = UNITS[unit] if isinstance(unit, str) else int(unit)
+        p.encoding = ENCODINGS["bitmap"]
+        out = (KcU128 * max(1, kk.size))()
+        check(lib().kc_count_multi(self._h, C.byref(p), _u32p(kk), kk.size, out))
+        return [out[i].value() for i in range(kk.size)]
+
     def count_local(self, k: int, unit="node", part: int = 8, mode="orient"):
         """Local counts (the reference's -m lkc): a list whose entry v is the
         number of k-cliques containing vertex v; binary encoding."""

@@ -89,6 +89,7 @@ SIGNATURES = {
     "kc_graph_get_peel": (i32, [C.c_void_p, P(u32), P(u32)]),
     "kc_count": (i32, [C.c_void_p, P(KcParams), P(KcU128), P(KcCountStats)]),
     "kc_count_shard": (i32, [C.c_void_p, P(KcParams), u32, u32, P(KcU128), P(KcCountStats)]),
+    "kc_count_multi": (i32, [C.c_void_p, P(KcParams), P(u32), u32, P(KcU128)]),
     "kc_count_local": (i32, [C.c_void_p, P(KcParams), P(KcU128), P(KcU128)]),
     "kc_parse_spec": (i32, [C.c_char_p, P(KcParams)]),
     "kc_kcore": (i32, [C.c_void_p, P(u32), P(u32)]),

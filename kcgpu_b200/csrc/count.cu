@@ -326,6 +326,10 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
     lp.k_max = k_max;
     lp.part = req.part ? req.part : auto_part(lp.mode, (lp.dcap + 31) / 32);
     lp.q = lp.mode == KC_MODE_ORIENT ? 0u : req.part;
+    if (req.nk) {  // several k: a full warp per walker, one lane per k
+      lp.part = 32u;
+      lp.q = 0u;
+    }
     lp.local = req.d_local != nullptr;
     lp.depth_boost = depth_boost;
     CountParams p;
@@ -343,7 +347,9 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
     p.local = req.d_local;
     p.vgraph = g->vgraph;
     p.gk = req.d_graph_k;
-    p.k0 = req.k;
+    p.k0 = req.nk ? k_max : req.k;
+    p.nk = req.nk;
+    for (uint32_t i = 0; i < req.nk && i < 32u; ++i) p.kset[i] = req.kset[i];
     p.out = d_out;
     p.binom = ctx->d_binom;
     p.binom_cols = ctx->bcols;
@@ -500,7 +506,7 @@ kc_status count_graph(kc_graph* g, const CountRequest& req, unsigned long long* 
     if (st != KC_OK) break;
     if (err == DEV_ERR_STACK && boost == 0 && req.mode != KC_MODE_ORIENT) {
       // a clique tree deeper than the fast stack: rerun with the full depth
-      KC_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long) * 2 * req.n_graphs, s));
+      KC_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long) * 2 * req.n_graphs * std::max(1u, req.nk), s));
       continue;
     }
     if (err) st = device_error_status(err);

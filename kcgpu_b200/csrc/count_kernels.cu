@@ -231,6 +231,18 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
   pt.pbase = (lane / p.P) * p.P;
   pt.pmask = p.P >= 32 ? 0xffffffffu : (((1u << p.P) - 1u) << pt.pbase);
   const uint32_t part = gt / p.P;
+  // Several k in one walk (pivoting, one graph, p.nk > 0): the walk goes to
+  // the largest k, and lane `plane` of every partition keeps the count of
+  // kset[plane]. A clique-tree node with `hold` held vertices, `drop` pivots
+  // and candidate set C adds sum_j C(drop, j) cliques(G[C], k - hold - j);
+  // for a given k that sum is closed once k - hold <= 2, so k is taken
+  // (closed) at the first node on a path where k - hold <= 2, and the node
+  // below a non-pivot step from a parent with k - hold = 3 is where k - hold
+  // first reaches 2. A k that is still open at a leaf (no candidates) adds
+  // C(drop, k - hold) there.
+  const bool mk = MODE == 1 && !LOCAL && p.nk != 0u;
+  const bool kon = mk && pt.plane < p.nk;
+  const uint32_t kl = kon ? p.kset[pt.plane] : 0u;
 
   uint32_t* sb = smem + (size_t)gib * p.group_words;
   uint32_t* gb = p.gbuf ? p.gbuf + (size_t)(blockIdx.x * gpb + gib) * p.gbuf_words : nullptr;
@@ -278,7 +290,12 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
     if (G == 32) __syncwarp(); else __syncthreads();
   };
   auto flush = [&]() {
-    if (pt.plane == 0 && acc != 0 && acc_graph != 0xffffffffu) atomic_add_u128(p.out + 2ull * acc_graph, acc);
+    if (mk) {
+      if (kon && acc != 0 && acc_graph != 0xffffffffu)
+        atomic_add_u128(p.out + 2ull * ((size_t)acc_graph * p.nk + pt.plane), acc);
+    } else if (pt.plane == 0 && acc != 0 && acc_graph != 0xffffffffu) {
+      atomic_add_u128(p.out + 2ull * acc_graph, acc);
+    }
     acc = 0;
   };
 
@@ -453,6 +470,16 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
             if (p.edge_units) atomic_add_u128(p.local + 2ull * p.col[unit], tot);
           }
         }
+        gsync();
+        continue;
+      }
+    } else if (mk) {
+      // several k: every k with k - hold0 <= 1 is closed at the unit (the
+      // unit is the clique, or one more vertex of S); the others need G[S]
+      const uint32_t hold0 = p.edge_units ? 2u : 1u;
+      const uint32_t r0 = kl - hold0;  // (wraps for kl < hold0: no contribution)
+      if (part == 0 && !helper && kon && r0 <= 1u) acc += (r0 == 0u) ? 1u : d;
+      if (d == 0u || k < hold0 + 2u || hold0 + d < max(p.kset[0], hold0 + 2u)) {
         gsync();
         continue;
       }
@@ -660,7 +687,21 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
     gsync();
     lap(1);
 
-    if (MODE == 1 && k == (p.edge_units ? 4u : 3u)) {
+    if (mk) {
+      // several k: the k with k - hold0 = 2 is the number of edges of G[S]
+      const uint32_t hold0 = p.edge_units ? 2u : 1u;
+      if (part == 0 && !helper) {
+        unsigned long long e2 = 0;  // twice the edges: the bitmap is symmetric
+        for (uint32_t j = pt.plane; j < d; j += pt.P)
+          for (uint32_t w = 0; w < W; ++w) e2 += __popc(B[j * Ws + w]);
+        for (uint32_t o = 1; o < pt.P; o <<= 1) e2 += __shfl_xor_sync(pt.pmask, e2, o);
+        if (kon && kl == hold0 + 2u) acc += e2 / 2u;
+      }
+      if (k <= hold0 + 2u) {
+        gsync();
+        continue;
+      }
+    } else if (MODE == 1 && k == (p.edge_units ? 4u : 3u)) {
       // k - hold0 = 2: the unit's count is the number of edges of G[S]; a
       // vertex of S is in as many of those cliques as it has neighbours in S
       if (part == 0 && !helper) {
@@ -867,7 +908,9 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
       const bool narrow = pt.P == 32u && W <= 32u;
       const bool lc = LOCAL;  // local (per-vertex) counts
       unsigned __int128 leaf_cnt = 0, leaf_pinc = 0;
-      auto enter = [&](uint32_t* F, uint32_t hold, uint32_t drop, bool own) -> bool {
+      // pchild: the node is its parent's pivot branch (same held vertices);
+      // otherwise it holds one vertex more than its parent
+      auto enter = [&](uint32_t* F, uint32_t hold, uint32_t drop, bool own, bool pchild) -> bool {
         uint32_t nc = 0, nzm = 0;
         if (narrow) {
           const uint32_t x = pt.plane < W ? F[pt.plane] : 0u;
@@ -883,17 +926,20 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
         // cliques that hold any one of its pivots
         leaf_cnt = 0;
         leaf_pinc = 0;
+        // several k: this lane's k is still open here if its k - hold was
+        // at least 3 at the parent
+        const bool kopen = kon && kl + (pchild ? 0u : 1u) >= hold + 3u;
         if (nc == 0u) {
           leaf_cnt = binom(drop, r);
           if (r >= 1u && drop >= 1u) leaf_pinc = binom(drop - 1u, r - 1u);
-          if (own) uacc += leaf_cnt;
+          if (own) uacc += mk ? (kopen ? binom(drop, kl - hold) : (unsigned __int128)0u) : leaf_cnt;
           return false;
         }
-        if (hold + drop + nc < k) return false;
-        if (r <= 1u) {
+        if (hold + drop + nc < (mk ? p.kset[0] : k)) return false;
+        if (r <= 1u) {  // (never with several k: an open k has k - hold >= 2 here)
           leaf_cnt = (r == 0u) ? (unsigned __int128)1u : (unsigned __int128)(nc + drop);
           leaf_pinc = (r == 1u && drop >= 1u) ? 1u : 0u;
-          if (own) uacc += leaf_cnt;
+          if (own && !mk) uacc += leaf_cnt;
           if (lc && own && r == 1u)  // each candidate c completes one clique
             for (uint32_t w = pt.plane; w < W; w += pt.P)
               for (uint32_t x = F[w]; x; x &= x - 1u) loc2_add(w * 32u + (uint32_t)__ffs(x) - 1u, 1u);
@@ -964,9 +1010,12 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
         if (r == 2u) {  // edges of G[F] + drop * |F| + C(drop, 2)
           leaf_cnt = (unsigned __int128)(esum / 2u) + (unsigned __int128)drop * nc + binom(drop, 2u);
           leaf_pinc = drop >= 1u ? (unsigned __int128)(nc + drop - 1u) : 0u;
-          if (own) uacc += leaf_cnt;
+          if (own) uacc += mk ? ((kopen && kl == hold + 2u) ? leaf_cnt : (unsigned __int128)0u) : leaf_cnt;
           return false;
         }
+        // several k: a smaller k that reaches k - hold = 2 here is closed here
+        if (mk && own && kopen && kl == hold + 2u)
+          uacc += (unsigned __int128)(esum / 2u) + (unsigned __int128)drop * nc + binom(drop, 2u);
         best = __reduce_max_sync(pt.pmask, best);
         const uint32_t piv = 0xffffu - (best & 0xffffu);
         // branch set: candidates outside N(piv), less the pivot itself, whose
@@ -1077,7 +1126,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
         uint32_t* F0 = frames;
         for (uint32_t w = pt.plane; w < W; w += pt.P) F0[w] = B[v * Ws + w] & ~(R0[w] & low_mask(v, w));
         __syncwarp(pt.pmask);
-        if (!enter(F0, hold, drop, own1)) {
+        if (!enter(F0, hold, drop, own1, v == p0)) {
           if (lc && own1 && pt.plane == 0) {
             const unsigned __int128 x = (v != p0) ? leaf_cnt : leaf_pinc;
             if (x) loc2_add(v, x);
@@ -1116,7 +1165,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
             }
             for (uint32_t w = pt.plane; w < W; w += pt.P) F[w] &= B[fp * Ws + w];
             __syncwarp(pt.pmask);
-            if (!enter(F, fh, fd + 1u, own)) {
+            if (!enter(F, fh, fd + 1u, own, true)) {
               if (lc) {
                 if (pt.plane == 0) {
                   if (own) fr_take(F);
@@ -1151,7 +1200,7 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
           __syncwarp(pt.pmask);
           if (pt.plane == 0) F[u >> 5] &= ~(1u << (u & 31u));  // later siblings exclude u
           __syncwarp(pt.pmask);
-          if (descend && enter(Fc, h2, fd, own)) {
+          if (descend && enter(Fc, h2, fd, own, false)) {
             if (lc) {
               if (pt.plane == 0) fr_open(Fc, u);
               __syncwarp(pt.pmask);

@@ -22,7 +22,9 @@ struct CountParams {
   uint32_t edge_roots;       // node units whose root branches are their out-edges (edge units grouped by source)
   const uint32_t* vgraph;    // graph of every rank label, or null
   const uint32_t* gk;        // k of every graph, or null
-  uint32_t k0;               // k when gk is null
+  uint32_t k0;               // k when gk is null (the largest k with several k)
+  uint32_t nk;               // several k in one walk (pivoting, one graph): how many, 0 = one k
+  uint32_t kset[32];         // the k values, ascending; out holds nk (lo, hi) pairs
   unsigned long long* out;   // (lo, hi) per graph
   const unsigned long long* binom;  // C(r, c) as (lo, hi), row stride binom_cols + 1
   uint32_t binom_cols;

@@ -439,6 +439,11 @@ kc_status kc_count(kc_graph* g, const kc_params* p, kc_u128* out, kc_count_stats
   return kc::count_on(g->ctx, g, p, out, stats);
 }
 
+kc_status kc_count_multi(kc_graph* g, const kc_params* p, const uint32_t* ks, uint32_t n_k, kc_u128* out) {
+  if (!g) return fail(KC_ERR_INVALID_ARG, "NULL argument");
+  return kc::count_multi_on(g->ctx, g, p, ks, n_k, out);
+}
+
 kc_status kc_count_shard(kc_graph* g, const kc_params* p, uint32_t shard, uint32_t n_shards, kc_u128* out,
                          kc_count_stats* stats) {
   if (!g) return fail(KC_ERR_INVALID_ARG, "NULL argument");
@@ -494,6 +499,64 @@ kc_status count_on(kc_ctx* run, kc_graph* g, const kc_params* p, kc_u128* out, k
   out->lo = h[0];
   out->hi = h[1];
   return st;
+}
+
+kc_status count_multi_on(kc_ctx* run, kc_graph* g, const kc_params* p, const uint32_t* ks, uint32_t n_k,
+                         kc_u128* out) {
+  if (!run || !g || !p || !ks || !out) return fail(KC_ERR_INVALID_ARG, "NULL argument");
+  if (n_k == 0 || n_k > 32) return fail(KC_ERR_INVALID_ARG, "%u values of k: between 1 and 32 per call", n_k);
+  if (p->unit > KC_UNIT_EDGE) return fail(KC_ERR_INVALID_ARG, "unknown unit");
+  if (p->encoding != KC_ENC_BITMAP)
+    return fail(KC_ERR_INVALID_ARG, "several k in one walk need the binary encoding");
+  for (uint32_t i = 0; i < n_k; ++i)
+    if (ks[i] < 1) return fail(KC_ERR_INVALID_ARG, "k must be >= 1");
+  if (g->oriented < 0) return fail(KC_ERR_NOT_ORIENTED, "call kc_orient before kc_count_multi");
+  if (run != g->ctx && run->device != g->ctx->device)
+    return fail(KC_ERR_INVALID_ARG, "a graph can only be counted by a context of its own device");
+  kc::CtxLock lock(run);
+  // k <= 2 need no walk; the others, ascending and without repeats, share one
+  std::vector<uint32_t> big;
+  for (uint32_t i = 0; i < n_k; ++i) {
+    out[i] = {0, 0};
+    if (ks[i] == 1) out[i].lo = g->n;
+    else if (ks[i] == 2) out[i].lo = g->m;
+    else big.push_back(ks[i]);
+  }
+  std::sort(big.begin(), big.end());
+  big.erase(std::unique(big.begin(), big.end()), big.end());
+  if (big.empty()) return KC_OK;
+  const uint32_t nb = (uint32_t)big.size();
+  cudaStream_t s = run->stream;
+  kc::DevTemps t(s);
+  unsigned long long* d_out = nullptr;
+  KC_CUDA(t.alloc(&d_out, 2 * sizeof(unsigned long long) * nb));
+  KC_CUDA(cudaMemsetAsync(d_out, 0, 2 * sizeof(unsigned long long) * nb, s));
+  kc::CountRequest req;
+  req.k = big.front();
+  req.k_max = big.back();
+  req.mode = KC_MODE_PIVOT;
+  req.unit = p->unit;
+  req.part = 0;
+  req.encoding = KC_ENC_BITMAP;
+  req.flags = 0;
+  req.ctx = run;
+  req.nk = nb;
+  for (uint32_t i = 0; i < nb; ++i) req.kset[i] = big[i];
+  kc_status st = kc::count_graph(g, req, d_out, nullptr);
+  std::vector<unsigned long long> h(2 * (size_t)nb, 0);
+  if (st == KC_OK) {
+    cudaError_t e = cudaMemcpyAsync(h.data(), d_out, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = kc::cuda_fail(e, "count readback", __FILE__, __LINE__);
+  }
+  if (st != KC_OK) return st;
+  for (uint32_t i = 0; i < n_k; ++i) {
+    if (ks[i] <= 2) continue;
+    const size_t j = (size_t)(std::lower_bound(big.begin(), big.end(), ks[i]) - big.begin());
+    out[i].lo = h[2 * j];
+    out[i].hi = h[2 * j + 1];
+  }
+  return KC_OK;
 }
 
 kc_status complete_for_sharing(kc_graph* g) {

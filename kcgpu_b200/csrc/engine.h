@@ -106,6 +106,10 @@ struct CountRequest {
   // unit shard: this count takes the units whose index inside their size
   // class is = shard (mod n_shards); the shards' counts add up to the whole
   uint32_t shard = 0, n_shards = 1;
+  // several k in one walk (pivoting, one graph): nk ascending values >= 3,
+  // d_out then holds nk (lo, hi) pairs; k is the smallest, k_max the largest
+  uint32_t nk = 0;
+  uint32_t kset[32] = {};
 };
 
 // Runs the counting stage; d_out holds n_graphs (lo, hi) pairs and must be zeroed.
@@ -115,6 +119,9 @@ kc_status count_graph(kc_graph* g, const CountRequest& req, unsigned long long* 
 // of the same device; the graph must be complete (see CountRequest::ctx).
 kc_status count_on(kc_ctx* run, kc_graph* g, const kc_params* p, kc_u128* out, kc_count_stats* stats,
                    uint32_t shard = 0, uint32_t n_shards = 1);
+// kc_count_multi run by the context `run` (see count_on).
+kc_status count_multi_on(kc_ctx* run, kc_graph* g, const kc_params* p, const uint32_t* ks, uint32_t n_k,
+                         kc_u128* out);
 // Completes an oriented graph for counting by other contexts: builds every
 // array a count could create lazily and waits for the graph's stream.
 kc_status complete_for_sharing(kc_graph* g);

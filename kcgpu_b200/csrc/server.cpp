@@ -10,8 +10,10 @@
 // and their kernels overlap on the device through the workers' streams. A
 // worker that takes a one-shot request also takes the other queued one-shot
 // requests that fit (up to 512 requests / 8M edges) and counts them in one
-// batched call. Results are exact integers, so a request's count is the same
-// alone and in any mix.
+// batched call; a worker that takes a request for a resident graph also takes
+// the other queued requests for that graph (up to 32) and answers them with
+// one walk for all their k. Results are exact integers, so a request's count
+// is the same alone and in any mix.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -167,6 +169,43 @@ void execute_batch(kc_server* s, kc_ctx* ctx, std::vector<std::shared_ptr<Reques
   }
 }
 
+// Requests for one resident graph queued together are answered by one
+// pivoting walk for all their k (kc_count_multi: the walk goes to the largest
+// k and takes each smaller k where it closes), instead of one walk each.
+void execute_resident_group(kc_server* s, kc_ctx* ctx, std::vector<std::shared_ptr<Request>>& rs) {
+  std::shared_ptr<Resident> res;
+  {
+    std::lock_guard<std::mutex> l(s->mu);
+    auto it = s->graphs.find(rs.front()->graph_id);
+    if (it != s->graphs.end()) res = it->second;
+  }
+  kc_status st = KC_OK;
+  std::vector<uint32_t> ks;
+  std::vector<kc_u128> out(rs.size(), kc_u128{0, 0});
+  kc_params p;
+  std::memset(&p, 0, sizeof(p));
+  if (!res) {
+    st = kc::fail(KC_ERR_INVALID_ARG, "graph %llu is not resident", (unsigned long long)rs.front()->graph_id);
+  } else {
+    uint32_t kmax = 0;
+    for (auto& r : rs) {
+      ks.push_back(r->k);
+      kmax = std::max(kmax, r->k);
+    }
+    p = choose(s, res->info, kmax);
+    p.mode = KC_MODE_PIVOT;
+    p.part = 32;
+    p.encoding = KC_ENC_BITMAP;
+    st = kc::count_multi_on(ctx, res->g, &p, ks.data(), (uint32_t)ks.size(), out.data());
+  }
+  for (size_t i = 0; i < rs.size(); ++i) {
+    rs[i]->res.count = st == KC_OK ? out[i] : kc_u128{0, 0};
+    rs[i]->res.params = p;
+    rs[i]->res.params.k = rs[i]->k;
+    rs[i]->res.status = st;
+  }
+}
+
 // Admission: the first queued request whose projected footprint fits next to
 // the resident graphs and the requests already running (any request when
 // nothing runs, so a request as large as the whole budget still starts).
@@ -211,6 +250,19 @@ void worker_main(kc_server* s, size_t wi) {
         rs.push_back(std::move(r));
       };
       take(pick);
+      // requests for the same resident graph queued anywhere behind it join
+      // it in one walk (at most 32 of them)
+      if (rs.front()->graph_id != 0) {
+        const uint64_t gid = rs.front()->graph_id;
+        size_t i = 0;
+        while (i < s->queue.size() && rs.size() < 32) {
+          const Request& r = *s->queue[i];
+          if (r.graph_id == gid && s->resident_bytes + s->inflight_bytes + r.footprint <= s->budget)
+            take(s->queue.begin() + (long)i);
+          else
+            ++i;
+        }
+      }
       // one-shot requests (k >= 3) queued anywhere behind it join it in one
       // batched call while they fit
       if (rs.front()->graph_id == 0 && rs.front()->k >= 3) {
@@ -226,6 +278,7 @@ void worker_main(kc_server* s, size_t wi) {
       }
     }
     if (rs.size() == 1) execute(s, ctx, *rs[0]);
+    else if (rs.front()->graph_id != 0) execute_resident_group(s, ctx, rs);
     else execute_batch(s, ctx, rs);
     {
       std::lock_guard<std::mutex> l(s->mu);
