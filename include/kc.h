@@ -270,6 +270,9 @@ typedef struct kc_batch_opts {
   kc_params fixed;        /* used when autotune == 0 (k ignored) */
   uint32_t use_graph;     /* 1 = replay the counting stage as a captured CUDA graph */
   uint32_t flags;         /* KC_FLAG_STATS: fill the traversal counters below */
+  const kc_params* graph_params;  /* NULL, or the method of every graph (n_graphs
+                                     entries, k ignored): used instead of the
+                                     autotuner and `fixed` */
 } kc_batch_opts;
 
 typedef struct kc_batch_stats {

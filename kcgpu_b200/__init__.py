@@ -450,13 +450,23 @@ def footprint_bytes(n_nodes: int, n_edges: int, max_out: int) -> int:
     return int(lib().kc_footprint_bytes(n_nodes, n_edges, max_out))
 
 
+def _params(d: dict) -> KcParams:
+    p = KcParams()
+    for key, table in (("mode", MODES), ("unit", UNITS), ("encoding", ENCODINGS)):
+        v = d.get(key, 0)
+        setattr(p, key, table[v] if isinstance(v, str) else int(v))
+    p.part = int(d.get("part", 0))
+    return p
+
+
 def batch_count(ctx: Context, src, dst, edge_off, n_nodes, ks, orientation="degree", autotune=True,
                 fixed: dict | None = None, use_graph=True, return_choice=False, return_stats=False,
-                device_ptrs: tuple | None = None):
+                device_ptrs: tuple | None = None, graph_params: list | None = None):
     """Counts a packed batch: graph i owns edges [edge_off[i], edge_off[i+1]).
 
     With device_ptrs=(d_src, d_dst) the edges are read from device memory of
-    the context's GPU (src/dst are then ignored)."""
+    the context's GPU (src/dst are then ignored). graph_params: a method per
+    graph (dicts of mode / unit / part / encoding) instead of the autotuner."""
     if device_ptrs is None:
         s, d = _as_u32(src), _as_u32(dst)
     off = np.ascontiguousarray(edge_off, dtype=np.uint64)
@@ -473,6 +483,9 @@ def batch_count(ctx: Context, src, dst, edge_off, n_nodes, ks, orientation="degr
         opts.fixed.unit = UNITS.get(fixed.get("unit", "node"), 0) if isinstance(fixed.get("unit"), str) else int(fixed.get("unit", 0))
         opts.fixed.part = int(fixed.get("part", 8))
         opts.fixed.encoding = ENCODINGS.get(fixed.get("encoding", "bitmap"), 0) if isinstance(fixed.get("encoding"), str) else int(fixed.get("encoding", 0))
+    if graph_params is not None:
+        gp = (KcParams * max(1, g))(*[_params(x) for x in graph_params])
+        opts.graph_params = C.cast(gp, C.c_void_p)
     counts = (KcU128 * g)()
     choice = (KcParams * g)()
     st = KcBatchStats()

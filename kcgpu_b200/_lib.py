@@ -44,7 +44,7 @@ class KcBatchGraph(C.Structure):
 
 class KcBatchOpts(C.Structure):
     _fields_ = [("orientation", u32), ("autotune", u32), ("fixed", KcParams), ("use_graph", u32),
-                ("flags", u32)]
+                ("flags", u32), ("graph_params", C.c_void_p)]
 
 
 class KcBatchStats(C.Structure):

@@ -238,7 +238,9 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, Input
   if (st == KC_OK) {
     for (uint32_t g = 0; g < G; ++g) {
       kc_params p;
-      if (!opts || opts->autotune) {
+      if (opts && opts->graph_params) {
+        p = opts->graph_params[g];
+      } else if (!opts || opts->autotune) {
         p = autotune(n_nodes[g], fm[g], fmax[g], ks[g], fcore[g], orientation);
       } else {
         p = opts->fixed;  // part 0: each size class sizes its own partitions
@@ -281,6 +283,7 @@ kc_status run_batch(kc_ctx* ctx, const uint32_t* src, const uint32_t* dst, Input
       req.d_graph_k = dk;
       req.n_graphs = G;
       req.k_max = kmax;
+      req.help = groups.size() == 1;  // passes side by side share the SMs
       plans.emplace_back();
       st = count_prepare(&U, req, dout, 0, &plans.back());
       if (st != KC_OK) break;
@@ -490,8 +493,13 @@ kc_status run_batch_pipelined(kc_ctx* ctx, const uint32_t* src, const uint32_t* 
     rel.resize((size_t)gn + 1);
     for (uint32_t i = 0; i <= gn; ++i) rel[i] = edge_off[g0 + i] - edge_off[g0];
     kc_batch_stats cs;
+    kc_batch_opts co;
+    if (opts) {
+      co = *opts;
+      if (co.graph_params) co.graph_params += g0;
+    }
     KC_TRY(run_batch(ctx, buf[c & 1][0], buf[c & 1][1], Input::kDeviceOwned, rel.data(), n_nodes + g0, ks + g0, gn,
-                     opts, counts + g0, choice ? choice + g0 : nullptr, stats ? &cs : nullptr));
+                     opts ? &co : nullptr, counts + g0, choice ? choice + g0 : nullptr, stats ? &cs : nullptr));
     if (!stats) continue;
     sum.ms_build += cs.ms_build;
     sum.ms_count += cs.ms_count;

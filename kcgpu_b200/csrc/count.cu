@@ -239,6 +239,11 @@ static kc_status ensure_side(kc_ctx* ctx) {
   return KC_OK;
 }
 
+kc_status warm_context(kc_ctx* ctx) {
+  KC_TRY(ensure_side(ctx));
+  return ensure_binom(ctx, 128, 34);
+}
+
 kc_status ensure_pass_streams(kc_ctx* ctx, size_t passes) {
   if (!ctx->pool_fork) KC_CUDA(cudaEventCreateWithFlags(&ctx->pool_fork, cudaEventDisableTiming));
   while (ctx->pool_done.size() < passes) {
@@ -290,7 +295,8 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
   // and 1, the heavy pass): a cut-node ticket per queue position (the class
   // queue, then the heavy list), an active-unit word per CTA per launch, and
   // the exited CTAs of each class launch.
-  const bool helping = req.mode != KC_MODE_ORIENT && req.encoding == KC_ENC_BITMAP && req.d_local == nullptr;
+  const bool helping = ctx->tail_help && req.help && req.mode != KC_MODE_ORIENT &&
+                       req.encoding == KC_ENC_BITMAP && req.d_local == nullptr;
   const size_t exit_at = 2 * (size_t)nu + (size_t)(kNumClasses + 1) * kHelpMaxGrid;
   if (helping) {
     pl->help_words = exit_at + kNumClasses;

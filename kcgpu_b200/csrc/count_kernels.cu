@@ -477,9 +477,12 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
       // several k: every k with k - hold0 <= 1 is closed at the unit (the
       // unit is the clique, or one more vertex of S); the others need G[S]
       const uint32_t hold0 = p.edge_units ? 2u : 1u;
+      // (into uacc: a unit that outruns its budget drops it with its walk,
+      // and the heavy pass counts the whole unit again)
       const uint32_t r0 = kl - hold0;  // (wraps for kl < hold0: no contribution)
-      if (part == 0 && !helper && kon && r0 <= 1u) acc += (r0 == 0u) ? 1u : d;
+      if (part == 0 && !helper && kon && r0 <= 1u) uacc += (r0 == 0u) ? 1u : d;
       if (d == 0u || k < hold0 + 2u || hold0 + d < max(p.kset[0], hold0 + 2u)) {
+        acc += uacc;
         gsync();
         continue;
       }
@@ -695,9 +698,10 @@ __global__ void __launch_bounds__(256, MODE == 0 ? 4 : 3) k_count_bitmap(CountPa
         for (uint32_t j = pt.plane; j < d; j += pt.P)
           for (uint32_t w = 0; w < W; ++w) e2 += __popc(B[j * Ws + w]);
         for (uint32_t o = 1; o < pt.P; o <<= 1) e2 += __shfl_xor_sync(pt.pmask, e2, o);
-        if (kon && kl == hold0 + 2u) acc += e2 / 2u;
+        if (kon && kl == hold0 + 2u) uacc += e2 / 2u;
       }
       if (k <= hold0 + 2u) {
+        acc += uacc;
         gsync();
         continue;
       }

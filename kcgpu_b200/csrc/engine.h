@@ -21,6 +21,11 @@ struct kc_ctx {
   // (0 = kc::kDefaultBatchChunkEdges, UINT64_MAX = never)
   uint64_t batch_chunk_edges = 0;
   cudaStream_t copy = nullptr;  // host->device copies of the batch pipeline (created on first use)
+  // Idle CTAs of a pivoting launch join units still being walked (tail
+  // helping). Off for a context that shares the GPU with other busy contexts
+  // (the server's workers): a helping grid holds its SMs until its last unit
+  // ends, which would stall the other contexts' launches.
+  bool tail_help = true;
   kc::BlockCache cache;        // device blocks reused by allocations on `stream`
   uint64_t total_mem = 0;
   std::mutex mu;  // one call at a time per context
@@ -86,6 +91,9 @@ kc_status build_csr(kc_graph* g, const uint32_t* d_src, const uint32_t* d_dst, u
                     uint32_t n_nodes);
 kc_status orient_graph(kc_graph* g, uint32_t orientation);
 kc_status ensure_edge_rows(kc_graph* g);
+// Creates a context's side streams and a first binomial table, so the first
+// count on it pays for neither.
+kc_status warm_context(kc_ctx* ctx);
 // Grows the context's pass streams to hold `passes` counting passes side by side.
 kc_status ensure_pass_streams(kc_ctx* ctx, size_t passes);
 kc_status peel_graph(kc_graph* g);  // fills prio / level / max_core
@@ -110,6 +118,9 @@ struct CountRequest {
   // d_out then holds nk (lo, hi) pairs; k is the smallest, k_max the largest
   uint32_t nk = 0;
   uint32_t kset[32] = {};
+  // tail helping for this pass (also needs kc_ctx::tail_help); off for the
+  // passes of a batch that run side by side, for the reason given there
+  bool help = true;
 };
 
 // Runs the counting stage; d_out holds n_graphs (lo, hi) pairs and must be zeroed.

@@ -342,6 +342,11 @@ kc_status kc_server_create(kc_ctx* ctx, const kc_server_opts* opts, kc_server** 
   for (uint32_t i = 0; i < nw; ++i) {
     kc_ctx* w = nullptr;
     kc_status st = kc_ctx_create(ctx->device, &w);
+    if (st == KC_OK) {
+      w->tail_help = nw == 1;  // several workers share the SMs (see kc_ctx::tail_help)
+      st = kc::warm_context(w);
+      if (st != KC_OK) kc_ctx_destroy(w);
+    }
     if (st != KC_OK) {
       for (auto* c : s->wctx) kc_ctx_destroy(c);
       delete s;

@@ -78,15 +78,20 @@ def test_admission_passes_a_blocked_head(ctx):
 
 def test_cancel_and_admission(ctx):
     s, d, n = kc.gen_rmat(13, 16, seed=1).arrays()
+    bs, bd, bn = kc.gen_rmat(15, 10, seed=2).arrays()
     with kc.Server(ctx, streams=1) as srv:
         gid = srv.put_graph(s, d, n)
+        # a long one-shot request holds the one worker; requests for the
+        # resident graph queue behind it (and later run as one walk)
+        busy = srv.submit_edges(bs, bd, bn, 12)
         tickets = [srv.submit(gid, 6) for _ in range(6)]
-        srv.cancel(tickets[-1])  # still queued behind the others on one slot
+        srv.cancel(tickets[-1])  # still queued
         with pytest.raises(kc.KCError) as e:
             srv.wait(tickets[-1])
         assert e.value.name == "KC_ERR_CANCELLED"
         counts = {srv.wait(t)["count"] for t in tickets[:-1]}
         assert counts == {_alone(ctx, s, d, n, 6)}
+        assert srv.wait(busy)["count"] == _alone(ctx, bs, bd, bn, 12)
     # a budget smaller than one graph's projected footprint is rejected up front
     with kc.Server(ctx, hbm_budget_bytes=1 << 20, streams=1) as srv:
         with pytest.raises(kc.KCError) as e:
@@ -95,3 +100,20 @@ def test_cancel_and_admission(ctx):
         with pytest.raises(kc.KCError) as e:
             srv.submit_edges(s, d, n, 4)
         assert e.value.name == "KC_ERR_ADMISSION"
+
+
+def test_queued_requests_of_a_resident_graph_share_one_walk(ctx):
+    """Requests for one resident graph that queue together run as one walk
+    for all their k (the same start and end), each with its own exact count."""
+    s, d, n = kc.gen_rmat(12, 12, seed=4).arrays()
+    bs, bd, bn = kc.gen_rmat(15, 10, seed=2).arrays()
+    ks = [3, 5, 7, 7, 9, 12, 15]
+    with kc.Server(ctx, streams=1) as srv:
+        gid = srv.put_graph(s, d, n)
+        busy = srv.submit_edges(bs, bd, bn, 12)  # holds the one worker meanwhile
+        tickets = [srv.submit(gid, k) for k in ks]
+        res = [srv.wait(t) for t in tickets]
+        srv.wait(busy)
+    assert len({(r["start_ms"], r["done_ms"]) for r in res}) == 1
+    for k, r in zip(ks, res):
+        assert r["count"] == _alone(ctx, s, d, n, k), k
