@@ -132,12 +132,15 @@ def autotune_leg(kc, ctx, s, d, off, nn, kk, choice, args):
         pass
     fixed = {"o8b-node": {"mode": "orient", "unit": "node", "part": 8, "encoding": "bitmap"},
              "p8b-node": {"mode": "pivot", "unit": "node", "part": 8, "encoding": "bitmap"}}
+    # and the fixed methods the sweep timed on its whole sample
     bf = sweep.get("best_fixed_method")
-    if bf:
-        code, unit = bf.split("-")
-        fixed[bf] = {"mode": {"o": "orient", "p": "pivot", "a": "auto"}[code[0]], "unit": unit,
-                     "part": 0 if code[1:-1] == "A" else int(code[1:-1]),
-                     "encoding": "bitmap" if code[-1] == "b" else "list"}
+    for name in [bf] + [n for n in sweep.get("whole_sample_ms", {}) if n != "table"]:
+        if not name or name in fixed:
+            continue
+        code, unit = name.split("-")
+        fixed[name] = {"mode": {"o": "orient", "p": "pivot", "a": "auto"}[code[0]], "unit": unit,
+                       "part": 0 if code[1:-1] == "A" else int(code[1:-1]),
+                       "encoding": "bitmap" if code[-1] == "b" else "list"}
     runs = {}
     ctx.set_time_limit(int(args.tune_time_limit * 1e9))
     try:
@@ -157,7 +160,7 @@ def autotune_leg(kc, ctx, s, d, off, nn, kk, choice, args):
         ctx.set_time_limit(0)
     done = [v["ms_count"] for k, v in runs.items() if k != "autotuned" and v["ms_count"] is not None]
     return {"choice_histogram": dict(hist.most_common()), "sample": f"first {P} graphs of the batch",
-            "counting_stage": runs, "sweep_best_fixed": bf,
+            "counting_stage": runs, "sweep_best_fixed": bf, "sweep_decision": sweep.get("decision"),
             "tuned_over_best_fixed": (min(done) / runs["autotuned"]["ms_count"]) if done else None}
 
 

@@ -114,6 +114,8 @@ def test_queued_requests_of_a_resident_graph_share_one_walk(ctx):
         tickets = [srv.submit(gid, k) for k in ks]
         res = [srv.wait(t) for t in tickets]
         srv.wait(busy)
-    assert len({(r["start_ms"], r["done_ms"]) for r in res}) == 1
+    # taken from the queue together (within a millisecond) and done together
+    assert len({r["done_ms"] for r in res}) == 1
+    assert max(r["start_ms"] for r in res) - min(r["start_ms"] for r in res) < 1.0
     for k, r in zip(ks, res):
         assert r["count"] == _alone(ctx, s, d, n, k), k
