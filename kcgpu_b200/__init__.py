@@ -450,6 +450,17 @@ def footprint_bytes(n_nodes: int, n_edges: int, max_out: int) -> int:
     return int(lib().kc_footprint_bytes(n_nodes, n_edges, max_out))
 
 
+def _u128_list(arr, n: int) -> list:
+    """Python ints from a ctypes array of kc_u128 (numpy for the common case
+    where no count needs the high word)."""
+    if n == 0:
+        return []
+    w = np.frombuffer(arr, dtype=np.uint64, count=2 * n).reshape(n, 2)
+    if not w[:, 1].any():
+        return w[:, 0].tolist()
+    return [(int(h) << 64) | int(lo) for lo, h in w.tolist()]
+
+
 def _params(d: dict) -> KcParams:
     p = KcParams()
     for key, table in (("mode", MODES), ("unit", UNITS), ("encoding", ENCODINGS)):
@@ -497,7 +508,7 @@ def batch_count(ctx: Context, src, dst, edge_off, n_nodes, ks, orientation="degr
         check(lib().kc_batch_count_packed_device(ctx.handle, C.c_void_p(device_ptrs[0]), C.c_void_p(device_ptrs[1]),
                                                  offp, _u32p(nn), _u32p(kk), g, C.byref(opts), counts, choice,
                                                  C.byref(st)))
-    res = [c.value() for c in counts]
+    res = _u128_list(counts, g)
     out = [res]
     if return_choice:
         out.append([{"mode": int(c.mode), "unit": int(c.unit), "part": int(c.part), "encoding": int(c.encoding)}

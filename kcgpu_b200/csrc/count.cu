@@ -366,7 +366,7 @@ kc_status count_prepare(kc_graph* g, const CountRequest& req, unsigned long long
     p.time_limit_ns = ctx->time_limit_ns;
     p.t0 = reinterpret_cast<const unsigned long long*>(pl->scratch + kStartWord);
     if (warp_group && budget_ok) {
-      p.budget = kUnitBudget;
+      p.budget = lp.mode == KC_MODE_PIVOT ? kPivotUnitBudget : kUnitBudget;
       p.heavy = pl->heavy;
       p.heavy_count = pl->scratch + kHeavyBounds + 1;
       any_budget = true;

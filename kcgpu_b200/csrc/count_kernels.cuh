@@ -104,6 +104,14 @@ void release_launch(PreparedLaunch& pl, cudaStream_t s);
 constexpr int kNumClasses = 4;
 constexpr uint32_t kWarpClassMax = 128;   // largest unit a warp group takes
 constexpr uint32_t kUnitBudget = 8192;    // traversal nodes before a warp unit is handed on
+#ifndef KC_PIVOT_UNIT_BUDGET
+#define KC_PIVOT_UNIT_BUDGET 2048
+#endif
+// the same for a warp unit walked by pivoting (a pivot node costs more: its
+// candidates are scored). Measured on R-MAT scale 16 (edge units, p8): k = 5
+// took 29.7 / 20.8 / 17.4 ms and k = 6 115 / 102 / 100 ms with 8192 / 2048 /
+// 1024; the serving mix was fastest with 2048.
+constexpr uint32_t kPivotUnitBudget = KC_PIVOT_UNIT_BUDGET;
 constexpr size_t kStaticSmemBytes = 64;
 constexpr uint32_t kHelpMaxGrid = 2048;   // most CTAs of a launch that takes part in tail helping   // static shared memory of the bitmap kernel (phase clocks), kept off the plan
 
