@@ -51,3 +51,29 @@ def test_chunked_batch_reports_bad_graph(ctx):
         assert kc.batch_count(ctx, s, d, off, nn, kk)  # the context is still usable
     finally:
         ctx.set_batch_chunk_edges(0)
+
+
+def test_per_graph_methods_given_by_the_caller(ctx):
+    """kc_batch_opts.graph_params: every graph on the method the caller names
+    (several passes side by side, in one pass and as a pipeline); the counts
+    equal the autotuned batch's and each graph reports its method."""
+    s, d, off, nn, kk = _batch()
+    methods = [{"mode": "pivot", "unit": "node", "part": 8, "encoding": "bitmap"},
+               {"mode": "orient", "unit": "edge", "part": 4, "encoding": "bitmap"},
+               {"mode": "auto", "unit": "node", "part": 32, "encoding": "list"},
+               {"mode": "pivot", "unit": "edge", "part": 0, "encoding": "list"}]
+    gp = [methods[i % len(methods)] for i in range(len(nn))]
+    try:
+        ctx.set_batch_chunk_edges(NEVER)
+        want = kc.batch_count(ctx, s, d, off, nn, kk)
+        for chunk in (NEVER, 5000):
+            ctx.set_batch_chunk_edges(chunk)
+            got, choice = kc.batch_count(ctx, s, d, off, nn, kk, graph_params=gp, return_choice=True)
+            assert got == want, chunk
+            for i, c in enumerate(choice):
+                m = gp[i]
+                if int(kk[i]) > 2:
+                    assert (c["mode"], c["unit"], c["part"], c["encoding"]) == (
+                        kc.MODES[m["mode"]], kc.UNITS[m["unit"]], m["part"], kc.ENCODINGS[m["encoding"]]), i
+    finally:
+        ctx.set_batch_chunk_edges(0)
