@@ -69,7 +69,7 @@ def parse():
     ap.add_argument("--time-limit", type=float, default=900.0,
                     help="single-graph legs: device time limit of one count in seconds (the count then reports "
                          "a timeout instead of a number)")
-    ap.add_argument("--requests", type=int, default=512)
+    ap.add_argument("--requests", type=int, default=2048)
     ap.add_argument("--rate", type=float, default=2000.0)
     ap.add_argument("--serve-max-edges", type=float, default=1e5)
     ap.add_argument("--streams", type=int, default=2, help="serving: worker contexts / streams")
