@@ -583,6 +583,8 @@ def main():
     e2e_val = None
     if not args.no_e2e:
         counts_h = None
+        for _ in range(args.warmup):  # the host path's own buffers (staging, copy stream)
+            run_host()
         barrier(pg, local)
         ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
         for i in range(args.steps):

@@ -140,12 +140,13 @@ const char* kc_status_string(kc_status s);
  * count runs to completion, src/main.cu:303-580). */
 kc_status kc_ctx_set_time_limit(kc_ctx* ctx, uint64_t ns);
 /* Host-input batches (kc_batch_count, kc_batch_count_packed) holding more
- * than `edges` edges are counted as a pipeline of chunks of whole graphs of
- * about `edges` edges each: while one chunk is built and counted, the next
- * chunk's edges are copied to the device on a second stream, so the
+ * than `edges` edges are counted as a pipeline of ceil(edges in the batch /
+ * `edges`) chunks of whole graphs of about equal size: while one chunk is
+ * built and counted, the next chunk's edges are copied to the device on a
+ * second stream, so the
  * host->device copy of all but the first chunk is hidden behind device work.
  * Counts and choices are the same as in one pass; kc_batch_stats add up the
- * chunks (ms_h2d is the copy stream's time). 0 = the default (96M edges),
+ * chunks (ms_h2d is the copy stream's time). 0 = the default (160M edges),
  * UINT64_MAX = never split. Device-input batches always run in one pass. */
 kc_status kc_ctx_set_batch_chunk_edges(kc_ctx* ctx, uint64_t edges);
 /* Device memory the context keeps for reuse: the engine's temporaries and the

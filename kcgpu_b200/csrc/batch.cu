@@ -439,9 +439,14 @@ kc_status run_batch_pipelined(kc_ctx* ctx, const uint32_t* src, const uint32_t* 
   const double t0 = now_ms();
   for (uint32_t g = 0; g < G; ++g)
     if (edge_off[g + 1] < edge_off[g]) return fail(KC_ERR_INVALID_ARG, "edge_off decreases at graph %u", g);
-  std::vector<uint32_t> cut{0};  // chunk c holds graphs [cut[c], cut[c + 1])
+  // ceil(E / chunk_edges) chunks of about equal edges; chunk c holds graphs
+  // [cut[c], cut[c + 1])
+  const uint64_t E = edge_off[G] - edge_off[0];
+  const uint64_t n_chunks = (E + chunk_edges - 1) / chunk_edges;
+  const uint64_t target = (E + n_chunks - 1) / n_chunks;
+  std::vector<uint32_t> cut{0};
   for (uint32_t g = 0; g + 1 < G; ++g)
-    if (edge_off[g + 1] - edge_off[cut.back()] >= chunk_edges) cut.push_back(g + 1);
+    if (edge_off[g + 1] - edge_off[cut.back()] >= target) cut.push_back(g + 1);
   cut.push_back(G);
   const uint32_t C = (uint32_t)cut.size() - 1;
   uint64_t max_chunk = 1;
