@@ -103,7 +103,10 @@ void release_launch(PreparedLaunch& pl, cudaStream_t s);
 // pass (CTA per unit) over the warp-class units that ran over budget.
 constexpr int kNumClasses = 4;
 constexpr uint32_t kWarpClassMax = 128;   // largest unit a warp group takes
-constexpr uint32_t kUnitBudget = 8192;    // traversal nodes before a warp unit is handed on
+#ifndef KC_UNIT_BUDGET
+#define KC_UNIT_BUDGET 8192
+#endif
+constexpr uint32_t kUnitBudget = KC_UNIT_BUDGET;  // traversal nodes before a warp unit is handed on
 #ifndef KC_PIVOT_UNIT_BUDGET
 #define KC_PIVOT_UNIT_BUDGET 2048
 #endif
