@@ -67,3 +67,44 @@ def test_sum_u128_over_two_gloo_ranks():
     got = sorted(q.get(timeout=10) for _ in range(2))
     want = [a + b for a, b in CASES]
     assert got == [(0, want), (1, want)]
+
+
+class _FakeGraph:
+    """Stands in for kcgpu_b200.Graph: shard i of S counts the units j with
+    j mod S == i of a fixed list of per-unit counts (as kc_count_shard deals
+    out the units of a size class)."""
+
+    UNITS = [3, 0, 7, 2**70, 5, 1, 9, 2**64 + 11, 4]
+
+    def count(self, k, shard=None, **params):
+        i, s = shard
+        return sum(c for j, c in enumerate(self.UNITS) if j % s == i)
+
+
+def _rank_sharded(rank: int, world: int, port: int, out):
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    sys.path.insert(0, str(ROOT))
+    from kcgpu_b200 import sharding as sh
+
+    out.put((rank, sh.count_sharded(_FakeGraph(), 5, mode="pivot")))
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_count_sharded_sums_every_unit_once(world):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_sharded, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    got = sorted(q.get(timeout=10) for _ in range(world))
+    assert got == [(r, sum(_FakeGraph.UNITS)) for r in range(world)]
